@@ -1,0 +1,204 @@
+/*
+ * hydroflux_gpu.h -- C ABI of the B200 (sm_100a) implementation of hydroflux
+ * solver-2d's explicit time step.
+ *
+ * Every entry point is `extern "C"`, takes plain pointers and sizes, and
+ * returns an int status (HF_OK = 0, negative on failure; the message is in
+ * hf_last_error()). Nothing here names a torch or CUDA C++ type: a CUDA
+ * stream is passed as `void*` (a cudaStream_t / CUstream handle, NULL for the
+ * legacy default stream).
+ *
+ * The surface mirrors the reference crate (franciscoparrao/hydroflux,
+ * crate hydroflux-solver-2d) so that a Rust `extern "C"` shim can sit behind
+ * its existing API:
+ *   - hf_sim_*    <-> `Simulation` (solver-2d/src/sim.rs:119-245)
+ *   - hf_cfl_time_step, hf_forward_euler_step, hf_ssprk2_step,
+ *     hf_manning_friction_step, hf_apply_rain, hf_apply_point_sources
+ *                 <-> the free functions re-exported at solver-2d/src/lib.rs:74-91
+ *   - hf_workspace_* <-> `StepWorkspace2D` (solver-2d/src/update.rs:743-777)
+ * Layout: the reference stores `Array2<Conserved2D>` (AoS {h,hu,hv}, row-major
+ * (n_rows, n_cols), row i along y, column j along x). Here the state is SoA:
+ * three row-major double arrays h, hu, hv of n_rows*n_cols; the hf_sim API
+ * also accepts/returns the AoS {h,hu,hv} layout of `Conserved2D`.
+ */
+#ifndef HYDROFLUX_GPU_H
+#define HYDROFLUX_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HF_ABI_VERSION 1
+
+/* Status codes. The first four mirror `SimError` (solver-2d/src/sim.rs:81-115). */
+enum hf_status_code {
+  HF_OK = 0,
+  HF_ERR_SHAPE_MISMATCH = -1, /* SimError::ShapeMismatch (sim.rs:83-91) */
+  HF_ERR_INVALID_CONFIG = -2, /* SimError::InvalidConfig (sim.rs:93-94) */
+  HF_ERR_DEGENERATE_DT = -3,  /* SimError::DegenerateDt (sim.rs:96-104) */
+  HF_ERR_STEP_BUDGET = -4,    /* SimError::StepBudgetExhausted (sim.rs:106-114) */
+  HF_ERR_NONFINITE = -5,      /* non-finite depth seen by the CFL reduction (opt-in) */
+  HF_ERR_TIMEOUT = -6,        /* a bounded device-side wait gave up */
+  HF_ERR_CUDA = -7,           /* CUDA runtime failure */
+  HF_ERR_INVALID_ARG = -8,    /* bad pointer / index; the reference panics here */
+  HF_ERR_OUT_OF_MEMORY = -9,  /* device allocation failed */
+  HF_ERR_UNSUPPORTED = -10    /* feature not available for this configuration */
+};
+
+/* Boundary kinds (solver-2d/src/boundary.rs:80-104). */
+enum hf_bc_kind {
+  HF_BC_TRANSMISSIVE = 0,
+  HF_BC_WALL = 1,
+  HF_BC_DISCHARGE = 2, /* value = q [m^2/s], coordinate-axis sign convention */
+  HF_BC_DEPTH = 3      /* value = h [m] */
+};
+
+/* Integrators (solver-2d/src/sim.rs:38-46). */
+enum hf_integrator { HF_FORWARD_EULER = 0, HF_SSPRK2 = 1 };
+
+typedef struct hf_boundary {
+  int32_t kind;  /* enum hf_bc_kind */
+  int32_t reserved;
+  double value;
+} hf_boundary;
+
+/* Boundaries2D (boundary.rs:131-140): same field order. */
+typedef struct hf_boundaries {
+  hf_boundary north; /* i = 0 */
+  hf_boundary south; /* i = n_rows - 1 */
+  hf_boundary west;  /* j = 0 */
+  hf_boundary east;  /* j = n_cols - 1 */
+} hf_boundaries;
+
+/* SimulationConfig (sim.rs:49-77) plus the friction threshold the driver
+ * passes to manning_friction_step (sim.rs:224, H_DRY) and an opt-in
+ * non-finite guard. */
+typedef struct hf_config {
+  double cfl;              /* (0, 1]; default 0.4 */
+  int32_t integrator;      /* enum hf_integrator; default HF_SSPRK2 */
+  int32_t check_finite;    /* 0 (default): reference behaviour; 1: HF_ERR_NONFINITE */
+  hf_boundaries boundaries;/* default: four walls */
+  uint64_t max_steps;      /* run_until budget; default 10,000,000 */
+  double max_dt;           /* default 60 s */
+  double friction_dry_tol; /* default 1e-6 (H_DRY) */
+} hf_config;
+
+/* Mesh2D (geometry.rs:31-47), host memory. */
+typedef struct hf_mesh_desc {
+  int64_t n_rows;
+  int64_t n_cols;
+  double dx;
+  double dy;
+  const double* bed;     /* n_rows*n_cols, row-major */
+  const double* manning; /* n_rows*n_cols, or NULL for manning_uniform everywhere */
+  double manning_uniform;
+} hf_mesh_desc;
+
+/* A device-resident mesh for the low-level entry points (caller-owned). */
+typedef struct hf_grid {
+  int64_t n_rows;
+  int64_t n_cols;
+  double dx;
+  double dy;
+  const double* bed;     /* device, n_rows*n_cols */
+  const double* manning; /* device, n_rows*n_cols (may be NULL when unused) */
+} hf_grid;
+
+/* Last error message of the calling thread ("" when none). */
+const char* hf_last_error(void);
+/* ABI version (HF_ABI_VERSION). */
+int hf_abi_version(void);
+/* Fills the reference defaults (SimulationConfig::default, sim.rs:67-77). */
+void hf_config_default(hf_config* cfg);
+
+/* ---------------------------------------------------------------------------
+ * Simulation handle (replaces `Simulation`, sim.rs:119-245). Owns device
+ * copies of the mesh and state, one CUDA stream and the step graphs. Not
+ * thread-safe: one caller thread per handle.
+ * ------------------------------------------------------------------------- */
+typedef struct hf_sim hf_sim;
+
+/* Simulation::new (sim.rs:130-165). h/hu/hv are host SoA arrays. */
+int hf_sim_create(const hf_mesh_desc* mesh, const double* h, const double* hu,
+                  const double* hv, const hf_config* cfg, int device, hf_sim** out);
+/* Same with the AoS {h,hu,hv} layout of Conserved2D. */
+int hf_sim_create_aos(const hf_mesh_desc* mesh, const double* hhuhv, const hf_config* cfg,
+                      int device, hf_sim** out);
+int hf_sim_destroy(hf_sim* sim);
+/* Simulation::step (sim.rs:204-228), then the attached forcings at t_new. */
+int hf_sim_step(hf_sim* sim, double dt_cap, double* dt_out);
+/* Simulation::run_until (sim.rs:231-245), forcings applied after every step. */
+int hf_sim_run_until(hf_sim* sim, double t_target);
+/* Simulation::time / steps (sim.rs:167-175). */
+int hf_sim_time(const hf_sim* sim, double* t);
+int hf_sim_steps(const hf_sim* sim, uint64_t* steps);
+/* Simulation::states / states_mut (sim.rs:177-186): host copies. */
+int hf_sim_get_state(hf_sim* sim, double* h, double* hu, double* hv);
+int hf_sim_set_state(hf_sim* sim, const double* h, const double* hu, const double* hv);
+int hf_sim_get_state_aos(hf_sim* sim, double* hhuhv);
+int hf_sim_set_state_aos(hf_sim* sim, const double* hhuhv);
+/* Simulation::set_boundaries (sim.rs:194-196). */
+int hf_sim_set_boundaries(hf_sim* sim, const hf_boundaries* bcs);
+/* Details of the last HF_ERR_DEGENERATE_DT / HF_ERR_STEP_BUDGET (the fields
+ * of SimError::DegenerateDt {dt,t,step} / StepBudgetExhausted {steps,t}). */
+int hf_sim_error_detail(const hf_sim* sim, double* dt, double* t, uint64_t* step);
+/* Device pointers of the resident state (valid until hf_sim_destroy) and the
+ * handle's stream, for zero-copy interop. */
+int hf_sim_device_state(hf_sim* sim, double** h, double** hu, double** hv, void** stream);
+/* Forcings applied after each step at t_new, in this order (the order of
+ * solver-2d/examples/uk_ea_test8a_official.rs:203-217):
+ *   apply_rain(rate(t_new), dt)          (source.rs:88-101)
+ *   apply_point_sources(Q_k(t_new), dt)  (source.rs:52-69)
+ * rate(t) and Q_k(t) are piecewise-linear series, held constant outside
+ * their first/last stamps; equal stamps make a step. n_points = 0 clears. */
+int hf_sim_set_rain(hf_sim* sim, int64_t n_points, const double* t, const double* rate);
+/* Source k has rows[k], cols[k] and the series t/q[offsets[k] .. offsets[k+1]). */
+int hf_sim_set_point_sources(hf_sim* sim, int64_t n_sources, const int64_t* rows,
+                             const int64_t* cols, const int64_t* offsets, const double* t,
+                             const double* q);
+
+/* ---------------------------------------------------------------------------
+ * Low-level entry points on caller-owned device buffers, mirroring the
+ * reference's free functions. All run on `stream` and are asynchronous
+ * unless they return a host value (hf_cfl_time_step synchronizes it).
+ * ------------------------------------------------------------------------- */
+typedef struct hf_workspace hf_workspace;
+/* StepWorkspace2D::new (update.rs:758): stage buffer + reduction scratch. */
+int hf_workspace_create(int64_t n_rows, int64_t n_cols, int device, hf_workspace** out);
+int hf_workspace_destroy(hf_workspace* ws);
+
+/* cfl_time_step (update.rs:148) when bcs == NULL, cfl_time_step_with_bcs
+ * (update.rs:170) otherwise. Writes +inf for a dry domain. */
+int hf_cfl_time_step(const hf_grid* grid, const double* h, const double* hu, const double* hv,
+                     const hf_boundaries* bcs, double cfl, hf_workspace* ws, void* stream,
+                     double* dt_out);
+/* forward_euler_step_with (update.rs:805): in place on h/hu/hv. */
+int hf_forward_euler_step(const hf_grid* grid, double* h, double* hu, double* hv,
+                          const hf_boundaries* bcs, double dt, hf_workspace* ws, void* stream);
+/* ssprk2_step_with (update.rs:1255): in place on h/hu/hv. */
+int hf_ssprk2_step(const hf_grid* grid, double* h, double* hu, double* hv,
+                   const hf_boundaries* bcs, double dt, hf_workspace* ws, void* stream);
+/* manning_friction_step (source.rs:130): reads grid->manning. */
+int hf_manning_friction_step(const hf_grid* grid, double* h, double* hu, double* hv, double dt,
+                             double dry_tol, void* stream);
+/* apply_rain (source.rs:88). */
+int hf_apply_rain(int64_t n_cells, double* h, double* hu, double* hv, double rate, double dt,
+                  void* stream);
+/* apply_point_sources (source.rs:52): rows/cols/q_mass are HOST arrays,
+ * applied in order (repeated cells accumulate like the reference's loop). */
+int hf_apply_point_sources(const hf_grid* grid, double* h, double* hu, double* hv,
+                           int64_t n_sources, const int64_t* rows, const int64_t* cols,
+                           const double* q_mass, double dt, void* stream);
+/* hllc_flux_x / hllc_flux_y (riemann.rs:80, 97) over n faces (device
+ * arrays, 3 doubles per state {h,hu,hv}, 3 per flux {mass,x_mom,y_mom}). */
+int hf_hllc_flux(int x_dir, int64_t n, const double* ul, const double* ur, double* flux,
+                 void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HYDROFLUX_GPU_H */
