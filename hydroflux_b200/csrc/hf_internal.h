@@ -1,0 +1,115 @@
+// hf_internal.h -- structures shared by the kernels and the C-ABI layer.
+#pragma once
+
+#include <cstdint>
+
+namespace hf {
+
+// Tile geometry of the fused stage kernel: a CTA advances a TX x TY block of
+// cells; its shared-memory halo is 4 cells (two-cell dry buffer of the
+// slope limiter + one neighbour slope + one neighbour alpha).
+constexpr int TX = 32;
+constexpr int TY = 16;
+constexpr int NTHREADS = 256;
+
+// Boundary descriptor in kernel arguments; sides in Boundaries2D order.
+struct BcDev {
+  int kind[4];    // north, south, west, east
+  double val[4];  // q for Discharge, h for Depth
+};
+
+enum CtrlMode { MODE_FIXED = 0, MODE_STEP = 1, MODE_RUN = 2 };
+
+// Device-resident step control block. dt, the simulation clock and the CFL
+// accumulators live here, so a step needs no host round trip.
+struct Ctrl {
+  double t;         // simulation time
+  double dt;        // dt of the step in flight
+  double t_new;     // t + dt
+  double t_target;  // MODE_RUN target
+  double dt_cap;    // MODE_STEP cap
+  double cfl;
+  double max_dt;
+  double rain_dh;   // rate(t_new) * dt
+  unsigned long long sx_bits;    // max |u| + c over the current state (bits of a double >= 0)
+  unsigned long long sy_bits;
+  unsigned long long nonfinite;  // cells with non-finite depth (opt-in check)
+  long long steps;
+  long long budget;  // MODE_RUN step budget left
+  int mode;
+  int active;        // 1 while the step in flight runs
+  int status;        // 0 or an hf_status_code
+  int rain_on;       // rate(t_new) != 0
+  int pending;       // MODE_STEP: one step requested
+  int check_finite;
+  int cfl_valid;     // accumulators describe the current state
+  int quiet_budget;  // MODE_RUN: an exhausted budget ends the run without error
+  double err_dt;
+  double err_t;
+  long long err_step;
+};
+
+// Forcing tables on the device (piecewise-linear series). Point sources are
+// bucketed by stage tile: sources of tile t are tile_order[tile_start[t] ..
+// tile_start[t+1]) in their original order.
+struct ForcingDev {
+  int n_rain;
+  int n_src;
+  const double* rain_t;
+  const double* rain_v;
+  const int* src_row;
+  const int* src_col;
+  const int* src_off;  // n_src + 1 offsets into src_t / src_q
+  const double* src_t;
+  const double* src_q;
+  const int* tile_start;
+  const int* tile_order;
+  double* src_dh;  // per source, set each step by the control kernel
+};
+
+struct StageArgs {
+  int nr, nc;
+  int tiles_x, tiles_y;
+  double dx, dy;
+  const double* z;
+  const double* n;
+  const double* in_h;
+  const double* in_hu;
+  const double* in_hv;
+  double* out_h;
+  double* out_hu;
+  double* out_hv;
+  const double* un_h;  // SSP-RK2 U^n (may alias out_*)
+  const double* un_hu;
+  const double* un_hv;
+  BcDev bc;
+  Ctrl* ctrl;
+  int combine;   // SSP-RK2 convex combination + floor with U^n
+  int finalize;  // friction + forcings + CFL reduction + clock commit
+  double dry_tol;
+  ForcingDev f;
+};
+
+// Launchers (hf_kernels.cu).
+int launch_stage(const StageArgs& a, int grid, void* stream);
+int launch_finalize(const StageArgs& a, int grid, void* stream);
+int launch_control(Ctrl* ctrl, double dx, double dy, const ForcingDev& f, void* stream);
+int launch_cfl(const StageArgs& a, int with_ghosts, int grid, void* stream);
+int launch_set_fixed(Ctrl* ctrl, double dt, void* stream);
+int launch_set_step(Ctrl* ctrl, double dt_cap, double cfl, double max_dt, int check_finite,
+                    void* stream);
+int launch_set_run(Ctrl* ctrl, double t_target, long long budget, double cfl, double max_dt,
+                   int check_finite, int quiet_budget, void* stream);
+int launch_friction(int64_t ncell, const double* n, double* h, double* hu, double* hv, double dt,
+                    double dry_tol, void* stream);
+int launch_rain(int64_t ncell, double* h, double* hu, double* hv, double rate, double dt,
+                void* stream);
+int launch_point_sources(int64_t nc, double* h, double* hu, double* hv, int n,
+                         const int64_t* rows, const int64_t* cols, const double* q, double dt,
+                         double dx, double dy, void* stream);
+int launch_hllc(int x_dir, int64_t n, const double* ul, const double* ur, double* out,
+                void* stream);
+int stage_grid_size(int tiles, int device);
+size_t stage_smem_bytes();
+
+}  // namespace hf

@@ -1,0 +1,162 @@
+"""Seeded synthetic workloads (no datasets: every input is generated).
+
+* `dam_break(n)` -- circular dam break: n x n, dx = 1 m, flat bed, h = 10 m
+  within 50 m of the centre and 1 m outside, n = 0.03, walls, CFL 0.5.
+* `valley(n, dx, seed)` -- flood in a synthetic valley: longitudinal slope
+  0.005 descending toward the south (outflow) side, side slopes
+  0.05 |x - x_c|, 200 Gaussian hills (height U[1, 20] m, sigma U[20, 200] m,
+  uniform centres), Manning n from 4 Voronoi land-cover patches over
+  {0.025, 0.035, 0.05, 0.08}, initially dry, one point inflow at the
+  upstream thalweg with a triangular hydrograph 0 -> peak at 30 min -> 0 at
+  60 min, rain 50 mm/h everywhere, transmissive (open) sides, CFL 0.5.
+
+Random numbers come from splitmix64 keyed by (seed, stream, index), so
+every generator is reproducible element by element.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import List, Optional, Tuple
+
+import numpy as np
+
+RAIN_50MM_H = 50.0e-3 / 3600.0
+MANNING_CLASSES = (0.025, 0.035, 0.05, 0.08)
+
+_M64 = (1 << 64) - 1
+
+
+def splitmix64(x: np.ndarray) -> np.ndarray:
+    """splitmix64 finalizer on uint64 arrays (wrapping arithmetic)."""
+    x = np.asarray(x, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        z = x + np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    return z
+
+
+def uniform(seed: int, stream: int, count: int, lo=0.0, hi=1.0) -> np.ndarray:
+    """`count` uniforms in [lo, hi) from (seed, stream)."""
+    key = (int(seed) * 0x100000001B3 + int(stream) * 0x9E3779B1) & _M64
+    idx = np.arange(count, dtype=np.uint64) + np.uint64(key)
+    bits = splitmix64(idx) >> np.uint64(11)
+    u = bits.astype(np.float64) * (1.0 / (1 << 53))
+    return lo + (hi - lo) * u
+
+
+@dataclass
+class Scenario:
+    """Mesh, initial state, boundaries and forcings of one solve."""
+    name: str
+    bed: np.ndarray
+    manning: np.ndarray
+    dx: float
+    dy: float
+    h: np.ndarray
+    hu: np.ndarray
+    hv: np.ndarray
+    bcs: Tuple = ((1, 0.0),) * 4  # (kind, value) north, south, west, east
+    cfl: float = 0.4
+    t_end: float = 0.0
+    max_dt: float = 60.0
+    rain: Optional[Tuple[np.ndarray, np.ndarray]] = None          # (t, rate)
+    sources: List[Tuple[int, int, np.ndarray, np.ndarray]] = field(default_factory=list)
+
+    @property
+    def shape(self):
+        return self.bed.shape
+
+    @property
+    def n_cells(self):
+        return int(self.bed.size)
+
+
+def dam_break(n: int = 256) -> Scenario:
+    xc = np.arange(n) + 0.5
+    X, Y = np.meshgrid(xc, xc)
+    r = np.sqrt((X - n / 2.0) ** 2 + (Y - n / 2.0) ** 2)
+    h = np.where(r < 50.0, 10.0, 1.0)
+    z = np.zeros((n, n))
+    return Scenario("dam_break", z, np.full_like(z, 0.03), 1.0, 1.0, h, np.zeros_like(h),
+                    np.zeros_like(h), bcs=((1, 0.0),) * 4, cfl=0.5, t_end=10.0)
+
+
+def valley_bed(n: int, dx: float, seed: int, n_hills: int = 200) -> np.ndarray:
+    L = n * dx
+    y = (np.arange(n) + 0.5) * dx  # along i (south = downstream)
+    x = (np.arange(n) + 0.5) * dx
+    bed = (0.005 * (L - y))[:, None] + (0.05 * np.abs(x - L / 2.0))[None, :]
+    amp = uniform(seed, 1, n_hills, 1.0, 20.0)
+    sig = uniform(seed, 2, n_hills, 20.0, 200.0)
+    cx = uniform(seed, 3, n_hills, 0.0, L)
+    cy = uniform(seed, 4, n_hills, 0.0, L)
+    for a, s, hx, hy in zip(amp, sig, cx, cy):
+        # Window of +-6 sigma (the Gaussian is below 1.6e-8 of its peak beyond).
+        r = 6.0 * s
+        j0, j1 = max(int((hx - r) / dx), 0), min(int((hx + r) / dx) + 1, n)
+        i0, i1 = max(int((hy - r) / dx), 0), min(int((hy + r) / dx) + 1, n)
+        if j0 >= j1 or i0 >= i1:
+            continue
+        gx = np.exp(-((x[j0:j1] - hx) ** 2) / (2.0 * s * s))
+        gy = np.exp(-((y[i0:i1] - hy) ** 2) / (2.0 * s * s))
+        bed[i0:i1, j0:j1] += a * np.outer(gy, gx)
+    return bed
+
+
+def voronoi_manning(n: int, dx: float, seed: int, classes=MANNING_CLASSES) -> np.ndarray:
+    L = n * dx
+    k = len(classes)
+    sx = uniform(seed, 5, k, 0.0, L)
+    sy = uniform(seed, 6, k, 0.0, L)
+    x = (np.arange(n) + 0.5) * dx
+    y = (np.arange(n) + 0.5) * dx
+    best = np.full((n, n), np.inf)
+    out = np.empty((n, n))
+    for c in range(k):
+        d = (y[:, None] - sy[c]) ** 2 + (x[None, :] - sx[c]) ** 2
+        m = d < best
+        best[m] = d[m]
+        out[m] = classes[c]
+    return out
+
+
+def triangular_hydrograph(peak: float, t_peak: float = 1800.0, t_end: float = 3600.0):
+    return np.array([0.0, t_peak, t_end]), np.array([0.0, peak, 0.0])
+
+
+def valley(n: int = 4096, dx: float = 5.0, seed: int = 0, peak: float = 500.0,
+           t_end: float = 3600.0, manning: Optional[np.ndarray] = None,
+           rain_rate: float = RAIN_50MM_H) -> Scenario:
+    bed = valley_bed(n, dx, seed)
+    man = voronoi_manning(n, dx, seed) if manning is None else manning
+    z0 = np.zeros((n, n))
+    t, q = triangular_hydrograph(peak)
+    sources = [(0, n // 2, t, q)]
+    rain = (np.array([0.0]), np.array([rain_rate]))
+    return Scenario(f"valley{n}", bed, man, dx, dx, z0, z0.copy(), z0.copy(),
+                    bcs=((0, 0.0),) * 4, cfl=0.5, t_end=t_end, rain=rain, sources=sources)
+
+
+def simulation_for(s: Scenario, device: int = 0, integrator=None):
+    """A hydroflux_b200.sim.Simulation set up with the scenario's forcings."""
+    from . import sim as S
+    cfg = S.SimulationConfig(cfl=s.cfl, boundaries=S.Boundaries2D(*[S.Boundary(k, v)
+                                                                    for k, v in s.bcs]),
+                             max_dt=s.max_dt)
+    if integrator is not None:
+        cfg.integrator = integrator
+    sm = S.Simulation(S.Mesh2D(s.bed, s.dx, s.dy, s.manning), (s.h, s.hu, s.hv), cfg, device)
+    if s.rain is not None:
+        sm.set_rain(np.stack(s.rain, axis=1))
+    if s.sources:
+        sm.set_point_sources([S.PointSource(r, c, np.stack([t, q], axis=1))
+                              for r, c, t, q in s.sources])
+    return sm
+
+
+def oracle_forcing(s: Scenario):
+    """The same forcings as the oracle's Forcing descriptor (test/bench use)."""
+    from oracle.oracle import Forcing
+    return Forcing(rain=s.rain, sources=s.sources)

@@ -132,6 +132,19 @@ int hf_sim_destroy(hf_sim* sim);
 int hf_sim_step(hf_sim* sim, double dt_cap, double* dt_out);
 /* Simulation::run_until (sim.rs:231-245), forcings applied after every step. */
 int hf_sim_run_until(hf_sim* sim, double t_target);
+/* Advances exactly n_steps steps with run_until semantics toward t_target
+ * (each dt is also capped by t_target - t), stopping early if t_target is
+ * reached or a step fails. Steps are replayed from CUDA-graph chunks with no
+ * host round trip between them; the clock is read back once at the end.
+ * No counterpart in the reference: its callers loop over Simulation::step
+ * (sim.rs:204) one step at a time. */
+int hf_sim_run_steps(hf_sim* sim, uint64_t n_steps, double t_target);
+/* hf_sim_run_steps with every kernel launched directly and CUDA events on the
+ * handle's stream around each stage kernel: returns the summed stage-kernel
+ * time [ms], the number of stage launches and the whole region's time [ms].
+ * Used to measure the stage kernel against its roofline. */
+int hf_sim_run_steps_timed(hf_sim* sim, uint64_t n_steps, double t_target, double* stage_ms,
+                           uint64_t* stage_launches, double* total_ms);
 /* Simulation::time / steps (sim.rs:167-175). */
 int hf_sim_time(const hf_sim* sim, double* t);
 int hf_sim_steps(const hf_sim* sim, uint64_t* steps);

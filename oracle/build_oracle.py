@@ -15,7 +15,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "hf_oracle_capi.cpp")
 HDRS = [os.path.join(HERE, "hf_oracle.hpp"),
-        os.path.join(HERE, "..", "include", "hydroflux_gpu.h")]
+        os.path.join(HERE, "..", "include", "hydroflux_gpu.h"),
+        os.path.join(HERE, "..", "hydroflux_b200", "csrc", "hf_pow.h")]
 OUT = os.path.join(HERE, "libhf_oracle.so")
 
 CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-shared", "-ffp-contract=off",

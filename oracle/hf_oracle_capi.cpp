@@ -149,6 +149,16 @@ int hfo_set_threads(int n) {
 #endif
 }
 
+// 0: libm pow (the reference's platform behaviour); 1: correctly rounded.
+int hfo_set_pow_mode(int mode) {
+  pow_mode() = mode ? 1 : 0;
+  return pow_mode();
+}
+
+double hfo_pow_cr(double x, int which) {
+  return which == 0 ? hfpow::pow_4_3(x) : hfpow::pow_3_5(x);
+}
+
 int hfo_get_threads(void) {
 #ifdef _OPENMP
   return omp_get_max_threads();

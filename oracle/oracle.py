@@ -36,7 +36,20 @@ def lib():
         _LIB = C.CDLL(path)
         _LIB.hfo_last_error.restype = C.c_char_p
         _LIB.hfo_series_eval.restype = C.c_double
+        _LIB.hfo_pow_cr.restype = C.c_double
+        _LIB.hfo_pow_cr.argtypes = [C.c_double, C.c_int]
     return _LIB
+
+
+def set_pow_mode(mode: str) -> None:
+    """'libm' (the reference's platform pow, default) or 'cr' (correctly
+    rounded x^fl(4/3) and x^fl(3/5), as the GPU kernels compute)."""
+    lib().hfo_set_pow_mode(1 if mode == "cr" else 0)
+
+
+def pow_cr(x: float, which: int) -> float:
+    """Correctly rounded x^fl(4/3) (which = 0) or x^fl(3/5) (which = 1)."""
+    return lib().hfo_pow_cr(float(x), int(which))
 
 
 class OracleError(RuntimeError):

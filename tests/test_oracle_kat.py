@@ -397,3 +397,39 @@ def test_series_eval(oracle):
     assert oracle.series_eval(t, v, 5.0) == 0.5
     assert oracle.series_eval(t, v, 10.0) == 5.0  # equal stamps: a step
     assert oracle.series_eval(t, v, 30.0) == 5.0
+
+
+# ---------------------------------------------------------- correctly rounded pow
+def _cr_pow_reference(x, c):
+    from decimal import Decimal, getcontext
+    getcontext().prec = 70
+    return float(Decimal(float(x)) ** Decimal(float(c)))
+
+
+def test_correctly_rounded_pow(oracle):
+    """hf_pow.h returns the double nearest x^fl(4/3) and x^fl(3/5)
+    (checked against 70-digit decimal arithmetic)."""
+    rng = np.random.default_rng(11)
+    xs = np.concatenate([10.0 ** rng.uniform(-9, 3, 1500), rng.uniform(0.5, 2.0, 500)])
+    for which, c in ((0, 4.0 / 3.0), (1, 3.0 / 5.0)):
+        bad = [x for x in xs if oracle.pow_cr(x, which) != _cr_pow_reference(x, c)]
+        assert not bad, f"misrounded for exponent {c}: {bad[:3]}"
+    assert oracle.pow_cr(0.0, 0) == 0.0 and math.isnan(oracle.pow_cr(-1.0, 0))
+    assert oracle.pow_cr(float("inf"), 0) == float("inf")
+
+
+@pytest.mark.parametrize("mode", ["libm", "cr"])
+def test_both_pow_modes_reproduce_reference_profiles(oracle, mode):
+    """The two pow modes differ by at most one rounding per call; both keep
+    every printed digit of the reference's MacDonald run (friction on every
+    cell, Discharge/Depth boundaries)."""
+    import os
+    from tests.test_oracle_golden import run_free_loop
+    golden = np.load(os.path.join(os.path.dirname(__file__), "golden", "reference_verif.npz"))
+    oracle.set_pow_mode(mode)
+    try:
+        c = cases.macdonald()
+        h, _, _ = run_free_loop(oracle, c)
+    finally:
+        oracle.set_pow_mode("libm")
+    assert np.array_equal(cases.golden_profile(c, h), golden["macdonald"])
