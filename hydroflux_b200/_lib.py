@@ -60,6 +60,9 @@ PROTOTYPES = {
     "hf_apply_point_sources": (C.c_int, [C.POINTER(abi.hf_grid), _VP, _VP, _VP, C.c_int64,
                                          _I64P, _I64P, _D, C.c_double, _VP]),
     "hf_hllc_flux": (C.c_int, [C.c_int, C.c_int64, _VP, _VP, _VP, _VP]),
+    "hf_ssprk2_step_noalloc": (C.c_int, [C.POINTER(abi.hf_grid), _VP, _VP, _VP,
+                                         C.POINTER(abi.hf_boundaries), C.c_double, C.c_int,
+                                         _VP]),
 }
 
 

@@ -106,6 +106,8 @@ void dfree(void* p) {
 
 }  // namespace
 
+int hf::record_error(int code, const char* msg) { return fail(code, msg ? msg : ""); }
+
 // ---------------------------------------------------------------- forcing
 struct ForcingHost {
   int n_rain = 0, n_src = 0;

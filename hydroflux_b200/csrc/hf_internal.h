@@ -112,4 +112,7 @@ int launch_hllc(int x_dir, int64_t n, const double* ul, const double* ur, double
 int stage_grid_size(int tiles, int device);
 size_t stage_smem_bytes();
 
+// Sets the calling thread's hf_last_error() message and returns `code`.
+int record_error(int code, const char* msg);
+
 }  // namespace hf

@@ -205,6 +205,26 @@ int hf_apply_rain(int64_t n_cells, double* h, double* hu, double* hv, double rat
 int hf_apply_point_sources(const hf_grid* grid, double* h, double* hu, double* hv,
                            int64_t n_sources, const int64_t* rows, const int64_t* cols,
                            const double* q_mass, double dt, void* stream);
+/* ssprk2_step without allocating: no counterpart in the reference (whose
+ * StepWorkspace2D is always caller-allocated host memory). Same result as
+ * hf_ssprk2_step, but the stage buffer and control block live in a fixed
+ * array inside this library instead of an hf_workspace, so the call never
+ * runs cudaMalloc/cudaFree. It is meant for callers that cannot allocate
+ * device memory: hosts that reserve nearly all GPU memory for their own
+ * caching allocator up front, and latency-critical loops that must not
+ * trigger the device-wide synchronization cudaMalloc/cudaFree can cause.
+ * - Grids of at most HF_NOALLOC_MAX_CELLS cells (larger: HF_ERR_INVALID_ARG).
+ *   The array costs every GPU that loads the library 24 MiB + 512 B, held
+ *   until the process exits.
+ * - The first call on a device resolves the array's device address
+ *   (cudaGetSymbolAddress, with `device` current); make that first call
+ *   before any stream capture.
+ * - All calls on a device share the array and see the previous call's
+ *   leftovers (the control block is cleared each call): calls whose GPU work
+ *   overlaps, e.g. on two streams, race. Serialize them. */
+#define HF_NOALLOC_MAX_CELLS (1 << 20)
+int hf_ssprk2_step_noalloc(const hf_grid* grid, double* h, double* hu, double* hv,
+                           const hf_boundaries* bcs, double dt, int device, void* stream);
 /* hllc_flux_x / hllc_flux_y (riemann.rs:80, 97) over n faces (device
  * arrays, 3 doubles per state {h,hu,hv}, 3 per flux {mass,x_mom,y_mom}). */
 int hf_hllc_flux(int x_dir, int64_t n, const double* ul, const double* ur, double* flux,
