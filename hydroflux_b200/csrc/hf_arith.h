@@ -1,0 +1,52 @@
+// hf_arith.h -- IEEE division and square root without the zero slow path.
+//
+// On the GPU, double division by a finite nonzero divisor runs ~3.4x slower
+// when the numerator is zero (measured: 356 vs 1,214 G div/s on B200), and the
+// shallow-water step divides zeros all the time: still water, zero tangential
+// velocity, flat stretches in the slope limiter, zero momentum in friction.
+// IEEE 754 fixes the result of those cases exactly: +-0 / b is the zero with
+// sign(a) xor sign(b), and sqrt(+-0) is +-0. These helpers return that value
+// directly and otherwise compute the correctly rounded a / b or sqrt(x), so
+// they are bit-identical to `/` and `sqrt` for every input. The division
+// itself never sees the zero numerator (it divides 1 / b on those lanes and
+// discards the quotient), so predicated code avoids the slow path too.
+#pragma once
+
+#include <cmath>
+#include <cstdint>
+
+#if defined(__CUDACC__)
+#define HF_ARITH_HD __host__ __device__ __forceinline__
+#else
+#define HF_ARITH_HD inline
+#endif
+
+namespace hfa {
+
+#if defined(__CUDA_ARCH__)
+HF_ARITH_HD double div_rn(double a, double b) {
+  const long long ia = __double_as_longlong(a), ib = __double_as_longlong(b);
+  const bool a_zero = (ia << 1) == 0;
+  const bool b_regular = ((ib >> 52) & 0x7ff) != 0x7ff && (ib << 1) != 0;
+  const bool shortcut = a_zero && b_regular;
+  const double q = (shortcut ? 1.0 : a) / b;
+  return shortcut ? __longlong_as_double((ia ^ ib) & (long long)0x8000000000000000ull) : q;
+}
+HF_ARITH_HD double sqrt_rn(double x) {
+  const bool zero = (__double_as_longlong(x) << 1) == 0;
+  const double s = sqrt(zero ? 1.0 : x);
+  return zero ? x : s;
+}
+// +-0 and finiteness from the bit pattern (integer pipe, not the FP64 pipe).
+HF_ARITH_HD bool is_zero(double x) { return (__double_as_longlong(x) << 1) == 0; }
+HF_ARITH_HD bool is_finite(double x) {
+  return ((__double_as_longlong(x) >> 52) & 0x7ff) != 0x7ff;
+}
+#else
+HF_ARITH_HD double div_rn(double a, double b) { return a / b; }
+HF_ARITH_HD double sqrt_rn(double x) { return std::sqrt(x); }
+HF_ARITH_HD bool is_zero(double x) { return x == 0.0; }
+HF_ARITH_HD bool is_finite(double x) { return std::isfinite(x); }
+#endif
+
+}  // namespace hfa

@@ -8,6 +8,7 @@
 
 #include <cstdint>
 
+#include "hf_arith.h"
 #include "hf_internal.h"
 #include "hf_pow.h"
 
@@ -54,9 +55,9 @@ __device__ __forceinline__ Ghost ghost_cell(int side, const BcDev& bc, double h,
   if (kind == BC_DISCHARGE && h < H_DRY) {
     // |bed_slope| along the normal (boundary.rs:241-271); |a-b| is exact in
     // either order, so the side-specific operand order does not matter.
-    const double slope_mag = fabs((z[c0] - z[c1]) / d_normal);
+    const double slope_mag = fabs(hfa::div_rn(z[c0] - z[c1], d_normal));
     if (slope_mag > DRY_INFLOW_SLOPE_THRESHOLD) {
-      const double h_n = hfpow::pow_3_5(nman[c0] * (fabs(val) / sqrt(slope_mag)));
+      const double h_n = hfpow::pow_3_5(nman[c0] * hfa::div_rn(fabs(val), sqrt(slope_mag)));
       g.h = fmin(h_n, DRY_INFLOW_H_MAX);
     }
   }
@@ -77,8 +78,8 @@ __device__ __forceinline__ void hllc_normal(double h_l, double qn_l, double qt_l
   }
   const double cl = wl ? sqrt(h_l * GRAVITY) : 0.0;
   const double cr = wr ? sqrt(h_r * GRAVITY) : 0.0;
-  const double un_l = wl ? qn_l / h_l : 0.0;
-  const double un_r = wr ? qn_r / h_r : 0.0;
+  const double un_l = wl ? hfa::div_rn(qn_l, h_l) : 0.0;
+  const double un_r = wr ? hfa::div_rn(qn_r, h_r) : 0.0;
   double sl, sr;
   if (wl && wr) {
     sl = fmin(un_l - cl, un_r - cr);
@@ -98,8 +99,9 @@ __device__ __forceinline__ void hllc_normal(double h_l, double qn_l, double qt_l
     left = false; star = false;
   } else {
     const double denom = h_r * (un_r - sr) - h_l * (un_l - sl);
-    s_star = fabs(denom) > 1.0e-12 ? (h_r * (un_r - sr) * sl - h_l * (un_l - sl) * sr) / denom
-                                   : (sl + sr) * 0.5;
+    s_star = fabs(denom) > 1.0e-12
+                 ? hfa::div_rn(h_r * (un_r - sr) * sl - h_l * (un_l - sl) * sr, denom)
+                 : (sl + sr) * 0.5;
     left = s_star >= 0.0;
     star = true;
   }
@@ -108,7 +110,7 @@ __device__ __forceinline__ void hllc_normal(double h_l, double qn_l, double qt_l
   const double qt = left ? qt_l : qt_r;
   const double un = left ? un_l : un_r;
   const bool wet = left ? wl : wr;
-  const double ut = wet ? qt / h : 0.0;
+  const double ut = wet ? hfa::div_rn(qt, h) : 0.0;
   double fm = 0.0, fn = 0.0, ft = 0.0;
   if (wet) {
     fm = qn;
@@ -120,7 +122,7 @@ __device__ __forceinline__ void hllc_normal(double h_l, double qn_l, double qt_l
     return;
   }
   const double s = left ? sl : sr;
-  const double hs = h * (s - un) / (s - s_star);
+  const double hs = hfa::div_rn(h * (s - un), s - s_star);
   o_m = fm + (hs - h) * s;
   o_n = fn + (hs * s_star - qn) * s;
   o_t = ft + (hs * ut - qt) * s;
@@ -139,12 +141,12 @@ __device__ __forceinline__ void wb_face(double hL, double qnL, double qtL, doubl
   const double hsR = fmax(hR + zf - z_max, 0.0);
   double unL = 0.0, utL = 0.0, unR = 0.0, utR = 0.0;
   if (hL > H_VEL) {
-    unL = qnL / hL;
-    utL = qtL / hL;
+    unL = hfa::div_rn(qnL, hL);
+    utL = hfa::div_rn(qtL, hL);
   }
   if (hR > H_VEL) {
-    unR = qnR / hR;
-    utR = qtR / hR;
+    unR = hfa::div_rn(qnR, hR);
+    utR = hfa::div_rn(qtR, hR);
   }
   double fm, fn, ft;
   hllc_normal(hsL, hsL * unL, hsL * utL, hsR, hsR * unR, hsR * utR, fm, fn, ft);
@@ -156,19 +158,25 @@ __device__ __forceinline__ void wb_face(double hL, double qnL, double qtL, doubl
   tang = ft;
 }
 
-// minmod(dl / d, dr / d) (update.rs:362-370) with one division. Division by
-// d > 0 keeps the sign and the weak order of the numerators, so the operand
-// selected here has the quotient the reference returns (when the quotients
-// tie, both are the same value). Operands small enough for the reference's
-// product of quotients to underflow take the literal path.
+// The reference's minmod(dl / d, dr / d) evaluated literally (update.rs:362-370).
+__device__ __noinline__ double minmod_literal(double dl, double dr, double d) {
+  const double a = hfa::div_rn(dl, d), b = hfa::div_rn(dr, d);
+  if (a * b <= 0.0) return 0.0;
+  return fabs(a) < fabs(b) ? a : b;
+}
+
+// minmod(dl / d, dr / d) with one division. Division by d > 0 keeps the sign
+// and the weak order of the numerators, so the operand selected here has the
+// quotient the reference returns (when the quotients tie, both are the same
+// value). A zero difference makes the reference's product of quotients +-0,
+// hence 0. Tiny or infinite operands, where the reference's product of
+// quotients could underflow or be NaN, take the literal path out of line.
 __device__ __forceinline__ double minmod_div(double dl, double dr, double d) {
-  if (fabs(dl) < 1.0e-140 || fabs(dr) < 1.0e-140) {
-    const double a = dl / d, b = dr / d;
-    if (a * b <= 0.0) return 0.0;
-    return fabs(a) < fabs(b) ? a : b;
-  }
+  const bool finite = hfa::is_finite(dl) && hfa::is_finite(dr);
+  if ((hfa::is_zero(dl) || hfa::is_zero(dr)) && finite) return 0.0;
+  if (!finite || fabs(dl) < 1.0e-140 || fabs(dr) < 1.0e-140) return minmod_literal(dl, dr, d);
   if (dl * dr <= 0.0) return 0.0;
-  return fabs(dl) < fabs(dr) ? dl / d : dr / d;
+  return hfa::div_rn(fabs(dl) < fabs(dr) ? dl : dr, d);
 }
 
 // Manning friction on one cell (source.rs:150-164); h^(4/3) correctly rounded.
@@ -177,10 +185,10 @@ __device__ __forceinline__ void friction_cell(double h, double& hu, double& hv, 
   if (h <= dry_tol) return;
   if (n == 0.0) return;
   const double dt_g = dt * GRAVITY;
-  const double speed = sqrt(hu * hu + hv * hv) / h;
-  const double factor = n * n * speed / hfpow::pow_4_3(h) * dt_g + 1.0;
-  hu = hu / factor;
-  hv = hv / factor;
+  const double speed = hfa::div_rn(hfa::sqrt_rn(hu * hu + hv * hv), h);
+  const double factor = hfa::div_rn(n * n * speed, hfpow::pow_4_3(h)) * dt_g + 1.0;
+  hu = hfa::div_rn(hu, factor);
+  hv = hfa::div_rn(hv, factor);
 }
 
 // Piecewise-linear series (same definition as the host forcing descriptor).
@@ -193,7 +201,7 @@ __device__ __forceinline__ double series_eval(const double* ts, const double* vs
     const int mid = (lo + hi) / 2;
     if (ts[mid] <= t) lo = mid; else hi = mid;
   }
-  const double w = (t - ts[lo]) / (ts[lo + 1] - ts[lo]);
+  const double w = hfa::div_rn(t - ts[lo], ts[lo + 1] - ts[lo]);
   return vs[lo] + (vs[lo + 1] - vs[lo]) * w;
 }
 
@@ -206,8 +214,8 @@ __device__ __forceinline__ void cell_speeds(double h, double hu, double hv, doub
     const double c = sqrt(GRAVITY * h);
     double u = 0.0, v = 0.0;
     if (h > H_VEL) {
-      u = hu / h;
-      v = hv / h;
+      u = hfa::div_rn(hu, h);
+      v = hfa::div_rn(hv, h);
     }
     sx = fmax(sx, fabs(u) + c);
     sy = fmax(sy, fabs(v) + c);
@@ -219,8 +227,8 @@ __device__ __forceinline__ void ghost_speeds(const Ghost& g, double& sx, double&
   const double h = g.h;
   if (h <= H_DRY) return;
   const double c = sqrt(GRAVITY * h);
-  const double u = g.hu / h;
-  const double v = g.hv / h;
+  const double u = hfa::div_rn(g.hu, h);
+  const double v = hfa::div_rn(g.hv, h);
   sx = fmax(sx, fabs(u) + c);
   sy = fmax(sy, fabs(v) + c);
 }

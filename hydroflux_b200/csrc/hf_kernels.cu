@@ -137,7 +137,7 @@ __device__ __forceinline__ void commit_clock(Ctrl* c) {
 }  // namespace
 
 // One forward-Euler stage (update.rs:805-1211) over a persistent tile loop.
-__global__ void __launch_bounds__(NTHREADS, 2) k_stage(const StageArgs A) {
+__global__ void __launch_bounds__(NTHREADS, HF_MIN_BLOCKS) k_stage(const StageArgs A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   StageSmem& S = *reinterpret_cast<StageSmem*>(smem_raw);
   Ctrl* ctrl = A.ctrl;
@@ -172,8 +172,8 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_stage(const StageArgs A) {
           zz = A.z[g];
           e = hh + zz;
           if (hh > H_VEL) {
-            uu = A.in_hu[g] / hh;
-            vv = A.in_hv[g] / hh;
+            uu = hfa::div_rn(A.in_hu[g], hh);
+            vv = hfa::div_rn(A.in_hv[g], hh);
           }
         }
         S.z[k3] = zz;
@@ -214,14 +214,14 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_stage(const StageArgs A) {
           const int c3 = i3(li, lj);
           if (ga == 0) {
             const int r3 = c3 + st3;
-            se = (S.eta[r3] - S.eta[c3]) / d;
-            su = (S.u[r3] - S.u[c3]) / d;
-            sv = (S.v[r3] - S.v[c3]) / d;
+            se = hfa::div_rn(S.eta[r3] - S.eta[c3], d);
+            su = hfa::div_rn(S.u[r3] - S.u[c3], d);
+            sv = hfa::div_rn(S.v[r3] - S.v[c3], d);
           } else if (ga == na - 1) {
             const int l3 = c3 - st3;
-            se = (S.eta[c3] - S.eta[l3]) / d;
-            su = (S.u[c3] - S.u[l3]) / d;
-            sv = (S.v[c3] - S.v[l3]) / d;
+            se = hfa::div_rn(S.eta[c3] - S.eta[l3], d);
+            su = hfa::div_rn(S.u[c3] - S.u[l3], d);
+            sv = hfa::div_rn(S.v[c3] - S.v[l3], d);
           } else {
             const int l3 = c3 - st3, r3 = c3 + st3;
             se = minmod_div(S.eta[c3] - S.eta[l3], S.eta[r3] - S.eta[c3], d);
@@ -348,7 +348,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_stage(const StageArgs A) {
       if (fb > 0.0) out = out + fb * dt_dy;
       if (ft < 0.0) out = out + (-ft) * dt_dy;
       const double avail = fmax(S.h[i4(li, lj)] - H_DRY, 0.0);
-      S.a[k] = (out > avail && out > 0.0) ? avail / out : 1.0;
+      S.a[k] = (out > avail && out > 0.0) ? hfa::div_rn(avail, out) : 1.0;
     }
     __syncthreads();
 
@@ -359,8 +359,8 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_stage(const StageArgs A) {
       src_hi = A.f.tile_start[tile + 1];
     }
 #pragma unroll 1
-    for (int q = 0; q < 2; ++q) {
-      const int li = (tid >> 5) + 8 * q, lj = tid & 31;
+    for (int q = 0; q < CELLS_PER_THREAD; ++q) {
+      const int li = tid / TX + ROWS_PER_PASS * q, lj = tid % TX;
       const int gi = gi0 + li, gj = gj0 + lj;
       if (gi >= nr || gj >= nc) continue;
       const int64_t g = (int64_t)gi * nc + gj;
@@ -419,13 +419,15 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_stage(const StageArgs A) {
         const double eta_right = gj + 1 < nc ? eta_cell + sex * (0.5 * dx) : eta_cell;
         const double hfl = fmax(eta_left - zfl, 0.0);
         const double hfr = fmax(eta_right - zfr, 0.0);
-        const double s_hu = (hfl + hfr) * ((eta_left - hfl) - (eta_right - hfr)) * (0.5 * GRAVITY) / dx;
+        const double s_hu =
+            hfa::div_rn((hfl + hfr) * ((eta_left - hfl) - (eta_right - hfr)) * (0.5 * GRAVITY), dx);
         const double sey = S.sye[isy(li, lj)];
         const double eta_top = gi > 0 ? eta_cell - sey * (0.5 * dy) : eta_cell;
         const double eta_bot = gi + 1 < nr ? eta_cell + sey * (0.5 * dy) : eta_cell;
         const double hft = fmax(eta_top - zft, 0.0);
         const double hfb = fmax(eta_bot - zfb, 0.0);
-        const double s_hv = (hft + hfb) * ((eta_top - hft) - (eta_bot - hfb)) * (0.5 * GRAVITY) / dy;
+        const double s_hv =
+            hfa::div_rn((hft + hfb) * ((eta_top - hft) - (eta_bot - hfb)) * (0.5 * GRAVITY), dy);
 
         if (new_h <= H_VEL) {
           nh = fmax(new_h, 0.0);  // moisture floor keeps the mass
@@ -487,8 +489,8 @@ __global__ void __launch_bounds__(NTHREADS) k_finalize(const StageArgs A) {
       src_lo = A.f.tile_start[tile];
       src_hi = A.f.tile_start[tile + 1];
     }
-    for (int q = 0; q < 2; ++q) {
-      const int gi = gi0 + (threadIdx.x >> 5) + 8 * q, gj = gj0 + (threadIdx.x & 31);
+    for (int q = 0; q < CELLS_PER_THREAD; ++q) {
+      const int gi = gi0 + threadIdx.x / TX + ROWS_PER_PASS * q, gj = gj0 + threadIdx.x % TX;
       if (gi >= A.nr || gj >= A.nc) continue;
       const int64_t g = (int64_t)gi * A.nc + gj;
       double h = A.in_h[g], hu = A.in_hu[g], hv = A.in_hv[g];
@@ -513,8 +515,8 @@ __global__ void __launch_bounds__(NTHREADS) k_cfl(const StageArgs A, int with_gh
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int tyi = tile / A.tiles_x;
     const int gi0 = tyi * TY, gj0 = (tile - tyi * A.tiles_x) * TX;
-    for (int q = 0; q < 2; ++q) {
-      const int gi = gi0 + (threadIdx.x >> 5) + 8 * q, gj = gj0 + (threadIdx.x & 31);
+    for (int q = 0; q < CELLS_PER_THREAD; ++q) {
+      const int gi = gi0 + threadIdx.x / TX + ROWS_PER_PASS * q, gj = gj0 + threadIdx.x % TX;
       if (gi >= A.nr || gj >= A.nc) continue;
       const int64_t g = (int64_t)gi * A.nc + gj;
       const double h = A.in_h[g], hu = A.in_hu[g], hv = A.in_hv[g];

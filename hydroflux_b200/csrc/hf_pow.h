@@ -22,6 +22,8 @@
 
 #include <cmath>
 
+#include "hf_arith.h"
+
 #if defined(__CUDACC__)
 #define HF_POW_HD __host__ __device__ __forceinline__
 #else
@@ -45,7 +47,7 @@ HF_POW_HD double pow_4_3(double x) {
   two_prod(r0, r0, p, e);  // r0^2 = p + e
   two_prod(p, r0, q, f);   // r0^3 = q + f + e*r0
   const double res = (x - q) - (f + e * r0);  // x - q is exact (q ~ x)
-  const double corr = res / (3.0 * p);        // Newton: cbrt(x) ~ r0 + corr
+  const double corr = hfa::div_rn(res, 3.0 * p);  // Newton: cbrt(x) ~ r0 + corr
   double a_hi, a_lo;
   two_prod(x, r0, a_hi, a_lo);
   a_lo = a_lo + x * corr;
@@ -70,7 +72,7 @@ HF_POW_HD double pow_3_5(double x) {
   two_prod(s4, r0, s5, f5);
   f5 = f5 + f4 * r0;        // r0^5 = s5 + f5
   const double res = (p3 - s5) + ((e3 + e2 * x) - f5);  // p3 - s5 is exact
-  const double corr = res / (5.0 * s4);                  // Newton on r^5 = x^3
+  const double corr = hfa::div_rn(res, 5.0 * s4);        // Newton on r^5 = x^3
   const double eps = 2.2204460492503131e-17;             // 2^-53 / 5
   return r0 + (corr - r0 * (eps * log(x)));
 }
