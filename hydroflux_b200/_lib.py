@@ -46,6 +46,13 @@ PROTOTYPES = {
                                       C.POINTER(_VP)]),
     "hf_sim_set_rain": (C.c_int, [_VP, C.c_int64, _D, _D]),
     "hf_sim_set_point_sources": (C.c_int, [_VP, C.c_int64, _I64P, _I64P, _I64P, _D, _D]),
+    "hf_batch_create": (C.c_int, [C.c_int64, C.POINTER(abi.hf_scenario_desc), C.c_int,
+                                  C.POINTER(_VP)]),
+    "hf_batch_destroy": (C.c_int, [_VP]),
+    "hf_batch_run": (C.c_int, [_VP, C.c_uint64, C.POINTER(C.c_int64)]),
+    "hf_batch_scenario_info": (C.c_int, [_VP, C.c_int64, _D, C.POINTER(C.c_uint64),
+                                         C.POINTER(C.c_int)]),
+    "hf_batch_get_state": (C.c_int, [_VP, C.c_int64, _VP, _VP, _VP]),
     "hf_workspace_create": (C.c_int, [C.c_int64, C.c_int64, C.c_int, C.POINTER(_VP)]),
     "hf_workspace_destroy": (C.c_int, [_VP]),
     "hf_cfl_time_step": (C.c_int, [C.POINTER(abi.hf_grid), _VP, _VP, _VP,

@@ -55,6 +55,16 @@ class hf_mesh_desc(C.Structure):
                 ("manning", C.POINTER(C.c_double)), ("manning_uniform", C.c_double)]
 
 
+class hf_scenario_desc(C.Structure):
+    _fields_ = [("mesh", hf_mesh_desc), ("h", C.POINTER(C.c_double)),
+                ("hu", C.POINTER(C.c_double)), ("hv", C.POINTER(C.c_double)),
+                ("cfg", hf_config), ("t_end", C.c_double), ("n_rain", C.c_int64),
+                ("rain_t", C.POINTER(C.c_double)), ("rain_rate", C.POINTER(C.c_double)),
+                ("n_sources", C.c_int64), ("src_rows", C.POINTER(C.c_int64)),
+                ("src_cols", C.POINTER(C.c_int64)), ("src_offsets", C.POINTER(C.c_int64)),
+                ("src_t", C.POINTER(C.c_double)), ("src_q", C.POINTER(C.c_double))]
+
+
 class hf_grid(C.Structure):
     _fields_ = [("n_rows", C.c_int64), ("n_cols", C.c_int64), ("dx", C.c_double),
                 ("dy", C.c_double), ("bed", C.c_void_p), ("manning", C.c_void_p)]

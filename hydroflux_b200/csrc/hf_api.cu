@@ -108,50 +108,108 @@ void dfree(void* p) {
 
 int hf::record_error(int code, const char* msg) { return fail(code, msg ? msg : ""); }
 
+BcDev hf::boundaries_dev(const hf_boundaries& b) { return to_bcdev(b); }
+
 // ---------------------------------------------------------------- forcing
-struct ForcingHost {
-  int n_rain = 0, n_src = 0;
-  double* d_rain_t = nullptr;
-  double* d_rain_v = nullptr;
-  int* d_row = nullptr;
-  int* d_col = nullptr;
-  int* d_off = nullptr;
-  double* d_st = nullptr;
-  double* d_sq = nullptr;
-  int* d_tile_start = nullptr;
-  int* d_tile_order = nullptr;
-  double* d_dh = nullptr;
-  void release_rain() {
-    dfree(d_rain_t);
-    dfree(d_rain_v);
-    d_rain_t = d_rain_v = nullptr;
-    n_rain = 0;
+void ForcingHost::release_rain() {
+  dfree(d_rain_t);
+  dfree(d_rain_v);
+  d_rain_t = d_rain_v = nullptr;
+  n_rain = 0;
+}
+
+void ForcingHost::release_src() {
+  for (void* p : {(void*)d_row, (void*)d_col, (void*)d_off, (void*)d_st, (void*)d_sq,
+                  (void*)d_tile_start, (void*)d_tile_order, (void*)d_dh})
+    dfree(p);
+  d_row = d_col = d_off = d_tile_start = d_tile_order = nullptr;
+  d_st = d_sq = d_dh = nullptr;
+  n_src = 0;
+}
+
+ForcingDev ForcingHost::dev() const {
+  ForcingDev f;
+  f.n_rain = n_rain;
+  f.n_src = n_src;
+  f.rain_t = d_rain_t;
+  f.rain_v = d_rain_v;
+  f.src_row = d_row;
+  f.src_col = d_col;
+  f.src_off = d_off;
+  f.src_t = d_st;
+  f.src_q = d_sq;
+  f.tile_start = d_tile_start;
+  f.tile_order = d_tile_order;
+  f.src_dh = d_dh;
+  return f;
+}
+
+int hf::forcing_set_rain(ForcingHost& f, int64_t n_points, const double* t, const double* rate) {
+  if (n_points < 0 || (n_points > 0 && (!t || !rate)))
+    return fail(HF_ERR_INVALID_ARG, "bad rain series");
+  for (int64_t k = 1; k < n_points; ++k)
+    if (!(t[k] >= t[k - 1])) return fail(HF_ERR_INVALID_ARG, "rain time stamps must be sorted");
+  f.release_rain();
+  if (n_points == 0) return HF_OK;
+  HF_TRY(dalloc(&f.d_rain_t, (size_t)n_points));
+  HF_TRY(dalloc(&f.d_rain_v, (size_t)n_points));
+  HF_CUDA(cudaMemcpy(f.d_rain_t, t, n_points * sizeof(double), cudaMemcpyHostToDevice));
+  HF_CUDA(cudaMemcpy(f.d_rain_v, rate, n_points * sizeof(double), cudaMemcpyHostToDevice));
+  f.n_rain = (int)n_points;
+  return HF_OK;
+}
+
+int hf::forcing_set_sources(ForcingHost& f, int64_t nr, int64_t nc, int tiles_x, int tiles_y,
+                            int64_t n_sources, const int64_t* rows, const int64_t* cols,
+                            const int64_t* offsets, const double* t, const double* q) {
+  if (n_sources < 0) return fail(HF_ERR_INVALID_ARG, "bad point sources");
+  if (n_sources > 0 && (!rows || !cols || !offsets || !t || !q))
+    return fail(HF_ERR_INVALID_ARG, "null point-source arrays");
+  for (int64_t k = 0; k < n_sources; ++k) {
+    if (rows[k] < 0 || rows[k] >= nr || cols[k] < 0 || cols[k] >= nc)
+      return fail(HF_ERR_INVALID_ARG, "point source outside the mesh");
+    if (offsets[k + 1] <= offsets[k] || offsets[k] < 0)
+      return fail(HF_ERR_INVALID_ARG, "each point source needs at least one (t, q) point");
+    for (int64_t p = offsets[k] + 1; p < offsets[k + 1]; ++p)
+      if (!(t[p] >= t[p - 1])) return fail(HF_ERR_INVALID_ARG, "source time stamps must be sorted");
   }
-  void release_src() {
-    for (void* p : {(void*)d_row, (void*)d_col, (void*)d_off, (void*)d_st, (void*)d_sq,
-                    (void*)d_tile_start, (void*)d_tile_order, (void*)d_dh})
-      dfree(p);
-    d_row = d_col = d_off = d_tile_start = d_tile_order = nullptr;
-    d_st = d_sq = d_dh = nullptr;
-    n_src = 0;
+  f.release_src();
+  if (n_sources == 0) return HF_OK;
+  const int ns = (int)n_sources;
+  const int npts = (int)offsets[ns];
+  std::vector<int> r(ns), c(ns), off(ns + 1);
+  for (int k = 0; k < ns; ++k) {
+    r[k] = (int)rows[k];
+    c[k] = (int)cols[k];
   }
-  ForcingDev dev() const {
-    ForcingDev f;
-    f.n_rain = n_rain;
-    f.n_src = n_src;
-    f.rain_t = d_rain_t;
-    f.rain_v = d_rain_v;
-    f.src_row = d_row;
-    f.src_col = d_col;
-    f.src_off = d_off;
-    f.src_t = d_st;
-    f.src_q = d_sq;
-    f.tile_start = d_tile_start;
-    f.tile_order = d_tile_order;
-    f.src_dh = d_dh;
-    return f;
-  }
-};
+  for (int k = 0; k <= ns; ++k) off[k] = (int)offsets[k];
+  // Bucket the sources by stage tile, keeping their order within a tile.
+  const int ntiles = tiles_x * tiles_y;
+  std::vector<int> start(ntiles + 1, 0), order(ns);
+  for (int k = 0; k < ns; ++k) start[(r[k] / TY) * tiles_x + c[k] / TX + 1]++;
+  for (int k = 0; k < ntiles; ++k) start[k + 1] += start[k];
+  std::vector<int> fill(start.begin(), start.end() - 1);
+  for (int k = 0; k < ns; ++k) order[fill[(r[k] / TY) * tiles_x + c[k] / TX]++] = k;
+  HF_TRY(dalloc(&f.d_row, ns));
+  HF_TRY(dalloc(&f.d_col, ns));
+  HF_TRY(dalloc(&f.d_off, ns + 1));
+  HF_TRY(dalloc(&f.d_st, npts));
+  HF_TRY(dalloc(&f.d_sq, npts));
+  HF_TRY(dalloc(&f.d_tile_start, ntiles + 1));
+  HF_TRY(dalloc(&f.d_tile_order, ns));
+  HF_TRY(dalloc(&f.d_dh, ns));
+  HF_CUDA(cudaMemcpy(f.d_row, r.data(), ns * sizeof(int), cudaMemcpyHostToDevice));
+  HF_CUDA(cudaMemcpy(f.d_col, c.data(), ns * sizeof(int), cudaMemcpyHostToDevice));
+  HF_CUDA(cudaMemcpy(f.d_off, off.data(), (ns + 1) * sizeof(int), cudaMemcpyHostToDevice));
+  HF_CUDA(cudaMemcpy(f.d_st, t, npts * sizeof(double), cudaMemcpyHostToDevice));
+  HF_CUDA(cudaMemcpy(f.d_sq, q, npts * sizeof(double), cudaMemcpyHostToDevice));
+  HF_CUDA(cudaMemcpy(f.d_tile_start, start.data(), (ntiles + 1) * sizeof(int),
+                     cudaMemcpyHostToDevice));
+  HF_CUDA(cudaMemcpy(f.d_tile_order, order.data(), ns * sizeof(int), cudaMemcpyHostToDevice));
+  HF_CUDA(cudaMemset(f.d_dh, 0, ns * sizeof(double)));
+  f.n_src = ns;
+  return HF_OK;
+}
 
 struct hf_sim {
   int device = 0;
@@ -334,6 +392,12 @@ void destroy_sim(hf_sim* s) {
 
 }  // namespace
 
+int hf::check_grid_config(const hf_config* cfg, int64_t nr, int64_t nc) {
+  HF_TRY(check_shape(nr, nc));
+  HF_TRY(validate_config(cfg));
+  return check_bcs(cfg->boundaries, nr, nc);
+}
+
 extern "C" {
 
 const char* hf_last_error(void) { return g_err.c_str(); }
@@ -472,12 +536,15 @@ int hf_sim_run_until(hf_sim* s, double t_target) {
       const double est = (t_target - s->t) / s->last_dt;
       which = est <= 1.5 ? 0 : (est <= 12.0 ? 1 : 2);
     }
+    const uint64_t steps_before = s->steps;
     HF_TRY(build_graph(s, which));
     HF_CUDA(cudaGraphLaunch(s->graphs[which], s->stream));
     HF_TRY(read_ctrl(s));
     HF_TRY(ctrl_status(s));
     if (s->h_ctrl->dt > 0.0) s->last_dt = s->h_ctrl->dt;
     if (!(s->t < t_target)) break;
+    if (s->steps == steps_before)  // a chunk that takes no step would repeat forever
+      return fail(HF_ERR_TIMEOUT, "run_until made no progress: no step was taken in a chunk");
   }
   return HF_OK;
 }
@@ -642,77 +709,22 @@ int hf_sim_device_state(hf_sim* s, double** h, double** hu, double** hv, void** 
 }
 
 int hf_sim_set_rain(hf_sim* s, int64_t n_points, const double* t, const double* rate) {
-  if (!s || n_points < 0 || (n_points > 0 && (!t || !rate)))
-    return fail(HF_ERR_INVALID_ARG, "bad rain series");
-  for (int64_t k = 1; k < n_points; ++k)
-    if (!(t[k] >= t[k - 1])) return fail(HF_ERR_INVALID_ARG, "rain time stamps must be sorted");
+  if (!s) return fail(HF_ERR_INVALID_ARG, "null handle");
   DeviceGuard guard(s->device);
   cudaStreamSynchronize(s->stream);
   drop_graphs(s);
-  s->forcing.release_rain();
-  if (n_points == 0) return HF_OK;
-  HF_TRY(dalloc(&s->forcing.d_rain_t, (size_t)n_points));
-  HF_TRY(dalloc(&s->forcing.d_rain_v, (size_t)n_points));
-  HF_CUDA(cudaMemcpy(s->forcing.d_rain_t, t, n_points * sizeof(double), cudaMemcpyHostToDevice));
-  HF_CUDA(cudaMemcpy(s->forcing.d_rain_v, rate, n_points * sizeof(double), cudaMemcpyHostToDevice));
-  s->forcing.n_rain = (int)n_points;
-  return HF_OK;
+  return forcing_set_rain(s->forcing, n_points, t, rate);
 }
 
 int hf_sim_set_point_sources(hf_sim* s, int64_t n_sources, const int64_t* rows,
                              const int64_t* cols, const int64_t* offsets, const double* t,
                              const double* q) {
-  if (!s || n_sources < 0) return fail(HF_ERR_INVALID_ARG, "bad point sources");
-  if (n_sources > 0 && (!rows || !cols || !offsets))
-    return fail(HF_ERR_INVALID_ARG, "null point-source arrays");
-  for (int64_t k = 0; k < n_sources; ++k) {
-    if (rows[k] < 0 || rows[k] >= s->nr || cols[k] < 0 || cols[k] >= s->nc)
-      return fail(HF_ERR_INVALID_ARG, "point source outside the mesh");
-    if (offsets[k + 1] <= offsets[k] || offsets[k] < 0)
-      return fail(HF_ERR_INVALID_ARG, "each point source needs at least one (t, q) point");
-    for (int64_t p = offsets[k] + 1; p < offsets[k + 1]; ++p)
-      if (!(t[p] >= t[p - 1])) return fail(HF_ERR_INVALID_ARG, "source time stamps must be sorted");
-  }
+  if (!s) return fail(HF_ERR_INVALID_ARG, "null handle");
   DeviceGuard guard(s->device);
   cudaStreamSynchronize(s->stream);
   drop_graphs(s);
-  s->forcing.release_src();
-  if (n_sources == 0) return HF_OK;
-  const int ns = (int)n_sources;
-  const int npts = (int)offsets[ns];
-  std::vector<int> r(ns), c(ns), off(ns + 1);
-  for (int k = 0; k < ns; ++k) {
-    r[k] = (int)rows[k];
-    c[k] = (int)cols[k];
-  }
-  for (int k = 0; k <= ns; ++k) off[k] = (int)offsets[k];
-  // Bucket the sources by stage tile, keeping their order within a tile.
-  const int ntiles = s->tiles_x * s->tiles_y;
-  std::vector<int> start(ntiles + 1, 0), order(ns);
-  for (int k = 0; k < ns; ++k) start[(r[k] / TY) * s->tiles_x + c[k] / TX + 1]++;
-  for (int k = 0; k < ntiles; ++k) start[k + 1] += start[k];
-  std::vector<int> fill(start.begin(), start.end() - 1);
-  for (int k = 0; k < ns; ++k) order[fill[(r[k] / TY) * s->tiles_x + c[k] / TX]++] = k;
-  ForcingHost& f = s->forcing;
-  HF_TRY(dalloc(&f.d_row, ns));
-  HF_TRY(dalloc(&f.d_col, ns));
-  HF_TRY(dalloc(&f.d_off, ns + 1));
-  HF_TRY(dalloc(&f.d_st, npts));
-  HF_TRY(dalloc(&f.d_sq, npts));
-  HF_TRY(dalloc(&f.d_tile_start, ntiles + 1));
-  HF_TRY(dalloc(&f.d_tile_order, ns));
-  HF_TRY(dalloc(&f.d_dh, ns));
-  HF_CUDA(cudaMemcpy(f.d_row, r.data(), ns * sizeof(int), cudaMemcpyHostToDevice));
-  HF_CUDA(cudaMemcpy(f.d_col, c.data(), ns * sizeof(int), cudaMemcpyHostToDevice));
-  HF_CUDA(cudaMemcpy(f.d_off, off.data(), (ns + 1) * sizeof(int), cudaMemcpyHostToDevice));
-  HF_CUDA(cudaMemcpy(f.d_st, t, npts * sizeof(double), cudaMemcpyHostToDevice));
-  HF_CUDA(cudaMemcpy(f.d_sq, q, npts * sizeof(double), cudaMemcpyHostToDevice));
-  HF_CUDA(cudaMemcpy(f.d_tile_start, start.data(), (ntiles + 1) * sizeof(int),
-                     cudaMemcpyHostToDevice));
-  HF_CUDA(cudaMemcpy(f.d_tile_order, order.data(), ns * sizeof(int), cudaMemcpyHostToDevice));
-  HF_CUDA(cudaMemset(f.d_dh, 0, ns * sizeof(double)));
-  f.n_src = ns;
-  return HF_OK;
+  return forcing_set_sources(s->forcing, s->nr, s->nc, s->tiles_x, s->tiles_y, n_sources, rows,
+                             cols, offsets, t, q);
 }
 
 // ------------------------------------------------------------ workspace

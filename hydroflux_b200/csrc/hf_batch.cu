@@ -1,0 +1,336 @@
+// hf_batch.cu -- ensembles of independent scenarios in one launch per stage.
+//
+// All scenarios' fields live in one allocation (8 SoA fields x total cells,
+// scenario k at offset off[k]); their tiles form one list, and a batch step
+// is [per-scenario control -> stage 1 over every tile -> stage 2 over every
+// tile -> per-scenario clock commit], replayed from CUDA graphs of 1, 8 and
+// 64 batch steps. A small scenario no longer leaves most of the GPU idle or
+// pays a launch per step: the persistent grid keeps every SM busy with tiles
+// from whichever scenarios are still running.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/hydroflux_gpu.h"
+#include "hf_internal.h"
+
+using namespace hf;
+
+namespace {
+
+int bfail(int code, const std::string& m) { return record_error(code, m.c_str()); }
+
+int bcuda(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return HF_OK;
+  cudaGetLastError();
+  return bfail(e == cudaErrorMemoryAllocation ? HF_ERR_OUT_OF_MEMORY : HF_ERR_CUDA,
+               std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define B_CUDA(call)                              \
+  do {                                            \
+    cudaError_t _e = (call);                      \
+    if (_e != cudaSuccess) return bcuda(_e, #call); \
+  } while (0)
+#define B_TRY(x)              \
+  do {                        \
+    int _rc = (x);            \
+    if (_rc != 0) return _rc; \
+  } while (0)
+
+struct Guard {
+  int prev = -1;
+  explicit Guard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~Guard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+const int kBatchChunk[3] = {1, 8, 64};
+
+}  // namespace
+
+struct hf_batch {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int n = 0;
+  int64_t total_cells = 0;
+  int total_tiles = 0;
+  int grid = 1;
+  double* buf = nullptr;
+  double *h = nullptr, *hu = nullptr, *hv = nullptr, *h1 = nullptr, *hu1 = nullptr,
+         *hv1 = nullptr, *z = nullptr, *nman = nullptr;
+  Ctrl* d_ctrl = nullptr;
+  Ctrl* h_ctrl = nullptr;
+  StageArgs* d_args1 = nullptr;
+  StageArgs* d_args2 = nullptr;
+  int* d_tile_scn = nullptr;
+  std::vector<ForcingHost> forcing;
+  std::vector<int64_t> off, nr, nc;
+  std::vector<double> t_end;
+  cudaGraphExec_t graphs[3] = {nullptr, nullptr, nullptr};
+};
+
+namespace {
+
+void destroy_batch(hf_batch* b) {
+  if (!b) return;
+  Guard g(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  for (auto& ge : b->graphs)
+    if (ge) cudaGraphExecDestroy(ge);
+  for (auto& f : b->forcing) {
+    f.release_rain();
+    f.release_src();
+  }
+  for (void* p : {(void*)b->buf, (void*)b->d_ctrl, (void*)b->d_args1, (void*)b->d_args2,
+                  (void*)b->d_tile_scn})
+    if (p) cudaFree(p);
+  if (b->h_ctrl) cudaFreeHost(b->h_ctrl);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+int enqueue_batch_step(hf_batch* b) {
+  if (launch_batch_control(b->d_ctrl, b->d_args1, b->n, b->stream)) return bcuda(cudaGetLastError(), "control");
+  if (launch_stage_batch(b->d_args1, b->d_tile_scn, b->total_tiles, b->grid, b->stream))
+    return bcuda(cudaGetLastError(), "stage 1");
+  if (launch_stage_batch(b->d_args2, b->d_tile_scn, b->total_tiles, b->grid, b->stream))
+    return bcuda(cudaGetLastError(), "stage 2");
+  if (launch_batch_commit(b->d_ctrl, b->n, b->stream)) return bcuda(cudaGetLastError(), "commit");
+  return HF_OK;
+}
+
+int build_batch_graph(hf_batch* b, int which) {
+  if (b->graphs[which]) return HF_OK;
+  cudaGraph_t graph = nullptr;
+  B_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = HF_OK;
+  for (int k = 0; k < kBatchChunk[which] && rc == HF_OK; ++k) rc = enqueue_batch_step(b);
+  cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
+  if (rc != HF_OK) {
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+  }
+  B_CUDA(e);
+  e = cudaGraphInstantiate(&b->graphs[which], graph, 0);
+  cudaGraphDestroy(graph);
+  B_CUDA(e);
+  return HF_OK;
+}
+
+long long total_steps(const hf_batch* b) {
+  long long k = 0;
+  for (int s = 0; s < b->n; ++s) k += b->h_ctrl[s].steps;
+  return k;
+}
+
+int64_t count_unfinished(const hf_batch* b) {
+  int64_t k = 0;
+  for (int s = 0; s < b->n; ++s)
+    if (b->h_ctrl[s].status == 0 && b->h_ctrl[s].t < b->t_end[s]) ++k;
+  return k;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hf_batch_create(int64_t n_scenarios, const hf_scenario_desc* sc, int device, hf_batch** out) {
+  if (!out || !sc || n_scenarios <= 0) return bfail(HF_ERR_INVALID_ARG, "bad arguments");
+  if (n_scenarios > (1 << 24)) return bfail(HF_ERR_INVALID_ARG, "too many scenarios");
+  *out = nullptr;
+  int64_t total = 0, tiles = 0;
+  for (int64_t k = 0; k < n_scenarios; ++k) {
+    const hf_scenario_desc& d = sc[k];
+    if (!d.mesh.bed || !d.h || !d.hu || !d.hv) return bfail(HF_ERR_INVALID_ARG, "null scenario arrays");
+    B_TRY(check_grid_config(&d.cfg, d.mesh.n_rows, d.mesh.n_cols));
+    if (d.cfg.integrator != HF_SSPRK2)
+      return bfail(HF_ERR_UNSUPPORTED, "ensembles run the SSP-RK2 integrator only");
+    if (!(d.mesh.dx > 0.0) || !(d.mesh.dy > 0.0))
+      return bfail(HF_ERR_INVALID_ARG, "dx and dy must be strictly positive");
+    const int64_t nc = d.mesh.n_rows * d.mesh.n_cols;
+    if (d.mesh.manning) {
+      for (int64_t c = 0; c < nc; ++c)
+        if (!(d.mesh.manning[c] >= 0.0))
+          return bfail(HF_ERR_INVALID_ARG, "Manning n must be non-negative at every cell");
+    } else if (!(d.mesh.manning_uniform >= 0.0)) {
+      return bfail(HF_ERR_INVALID_ARG, "Manning n must be non-negative");
+    }
+    total += nc;
+    tiles += ((d.mesh.n_cols + TX - 1) / TX) * ((d.mesh.n_rows + TY - 1) / TY);
+  }
+  if (tiles > INT_MAX / 2) return bfail(HF_ERR_INVALID_ARG, "ensemble too large");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+    cudaGetLastError();
+    return bfail(HF_ERR_CUDA, "no such CUDA device");
+  }
+  Guard guard(device);
+  hf_batch* b = new hf_batch();
+  auto done = [&](int code) {
+    if (code != HF_OK) destroy_batch(b);
+    return code;
+  };
+  b->device = device;
+  b->n = (int)n_scenarios;
+  b->total_cells = total;
+  b->total_tiles = (int)tiles;
+  b->grid = stage_grid_size(b->total_tiles, device);
+  b->forcing.resize(b->n);
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return done(bcuda(cudaGetLastError(), "cudaStreamCreate"));
+  if (cudaMalloc((void**)&b->buf, 8 * (size_t)total * sizeof(double)) != cudaSuccess)
+    return done(bcuda(cudaGetLastError(), "cudaMalloc(ensemble fields)"));
+  double* f = b->buf;
+  b->h = f; b->hu = f + total; b->hv = f + 2 * total; b->h1 = f + 3 * total;
+  b->hu1 = f + 4 * total; b->hv1 = f + 5 * total; b->z = f + 6 * total; b->nman = f + 7 * total;
+  if (cudaMalloc((void**)&b->d_ctrl, b->n * sizeof(Ctrl)) != cudaSuccess ||
+      cudaMalloc((void**)&b->d_args1, b->n * sizeof(StageArgs)) != cudaSuccess ||
+      cudaMalloc((void**)&b->d_args2, b->n * sizeof(StageArgs)) != cudaSuccess ||
+      cudaMalloc((void**)&b->d_tile_scn, b->total_tiles * sizeof(int)) != cudaSuccess ||
+      cudaMallocHost((void**)&b->h_ctrl, b->n * sizeof(Ctrl)) != cudaSuccess)
+    return done(bcuda(cudaGetLastError(), "cudaMalloc(ensemble tables)"));
+  std::vector<StageArgs> a1(b->n), a2(b->n);
+  std::vector<int> tile_scn(b->total_tiles);
+  std::memset(b->h_ctrl, 0, b->n * sizeof(Ctrl));
+  int64_t o = 0;
+  int tb = 0;
+  for (int s = 0; s < b->n; ++s) {
+    const hf_scenario_desc& d = sc[s];
+    const int64_t nr = d.mesh.n_rows, nc = d.mesh.n_cols, ncell = nr * nc;
+    const size_t bytes = (size_t)ncell * sizeof(double);
+    b->off.push_back(o);
+    b->nr.push_back(nr);
+    b->nc.push_back(nc);
+    b->t_end.push_back(d.t_end);
+    if (cudaMemcpy(b->z + o, d.mesh.bed, bytes, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(b->h + o, d.h, bytes, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(b->hu + o, d.hu, bytes, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(b->hv + o, d.hv, bytes, cudaMemcpyHostToDevice) != cudaSuccess)
+      return done(bcuda(cudaGetLastError(), "upload scenario"));
+    if (d.mesh.manning) {
+      if (cudaMemcpy(b->nman + o, d.mesh.manning, bytes, cudaMemcpyHostToDevice) != cudaSuccess)
+        return done(bcuda(cudaGetLastError(), "upload manning"));
+    } else {
+      std::vector<double> nn((size_t)ncell, d.mesh.manning_uniform);
+      if (cudaMemcpy(b->nman + o, nn.data(), bytes, cudaMemcpyHostToDevice) != cudaSuccess)
+        return done(bcuda(cudaGetLastError(), "upload manning"));
+    }
+    const int tx = (int)((nc + TX - 1) / TX), ty = (int)((nr + TY - 1) / TY);
+    int rc = forcing_set_rain(b->forcing[s], d.n_rain, d.rain_t, d.rain_rate);
+    if (rc == HF_OK)
+      rc = forcing_set_sources(b->forcing[s], nr, nc, tx, ty, d.n_sources, d.src_rows, d.src_cols,
+                               d.src_offsets, d.src_t, d.src_q);
+    if (rc != HF_OK) return done(rc);
+    Ctrl& c = b->h_ctrl[s];
+    c.cfl = d.cfg.cfl;
+    c.max_dt = d.cfg.max_dt;
+    c.check_finite = d.cfg.check_finite;
+    c.mode = MODE_RUN;
+    c.t_target = d.t_end;
+    c.budget = d.cfg.max_steps > (uint64_t)LLONG_MAX ? LLONG_MAX : (long long)d.cfg.max_steps;
+    StageArgs& x = a1[s];
+    std::memset(&x, 0, sizeof x);
+    x.nr = (int)nr;
+    x.nc = (int)nc;
+    x.tiles_x = tx;
+    x.tiles_y = ty;
+    x.tile_base = tb;
+    x.dx = d.mesh.dx;
+    x.dy = d.mesh.dy;
+    x.z = b->z + o;
+    x.n = b->nman + o;
+    x.bc = boundaries_dev(d.cfg.boundaries);
+    x.ctrl = b->d_ctrl + s;
+    x.dry_tol = d.cfg.friction_dry_tol;
+    x.f = b->forcing[s].dev();
+    StageArgs y = x;
+    x.in_h = b->h + o; x.in_hu = b->hu + o; x.in_hv = b->hv + o;
+    x.out_h = b->h1 + o; x.out_hu = b->hu1 + o; x.out_hv = b->hv1 + o;
+    x.un_h = b->h + o; x.un_hu = b->hu + o; x.un_hv = b->hv + o;
+    y.in_h = b->h1 + o; y.in_hu = b->hu1 + o; y.in_hv = b->hv1 + o;
+    y.out_h = b->h + o; y.out_hu = b->hu + o; y.out_hv = b->hv + o;
+    y.un_h = b->h + o; y.un_hu = b->hu + o; y.un_hv = b->hv + o;
+    y.combine = 1;
+    y.finalize = 1;
+    a2[s] = y;
+    for (int t = 0; t < tx * ty; ++t) tile_scn[tb + t] = s;
+    tb += tx * ty;
+    o += ncell;
+  }
+  if (cudaMemcpy(b->d_args1, a1.data(), b->n * sizeof(StageArgs), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(b->d_args2, a2.data(), b->n * sizeof(StageArgs), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(b->d_tile_scn, tile_scn.data(), b->total_tiles * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(b->d_ctrl, b->h_ctrl, b->n * sizeof(Ctrl), cudaMemcpyHostToDevice) != cudaSuccess)
+    return done(bcuda(cudaGetLastError(), "upload ensemble tables"));
+  // CFL accumulators of every scenario from its initial state (with ghosts).
+  if (launch_cfl_batch(b->d_args1, b->d_tile_scn, b->total_tiles, b->grid, b->stream))
+    return done(bcuda(cudaGetLastError(), "initial CFL"));
+  if (cudaStreamSynchronize(b->stream) != cudaSuccess)
+    return done(bcuda(cudaGetLastError(), "initial CFL"));
+  *out = b;
+  return HF_OK;
+}
+
+int hf_batch_destroy(hf_batch* b) {
+  destroy_batch(b);
+  return HF_OK;
+}
+
+int hf_batch_run(hf_batch* b, uint64_t max_batch_steps, int64_t* n_unfinished) {
+  if (!b) return bfail(HF_ERR_INVALID_ARG, "null handle");
+  Guard guard(b->device);
+  uint64_t left = max_batch_steps;
+  B_CUDA(cudaMemcpyAsync(b->h_ctrl, b->d_ctrl, b->n * sizeof(Ctrl), cudaMemcpyDeviceToHost, b->stream));
+  B_CUDA(cudaStreamSynchronize(b->stream));
+  int64_t running = count_unfinished(b);
+  while (left > 0 && running > 0) {
+    const int which = left >= 64 ? 2 : (left >= 8 ? 1 : 0);
+    const long long steps_before = total_steps(b);
+    B_TRY(build_batch_graph(b, which));
+    B_CUDA(cudaGraphLaunch(b->graphs[which], b->stream));
+    left -= (uint64_t)kBatchChunk[which];
+    B_CUDA(cudaMemcpyAsync(b->h_ctrl, b->d_ctrl, b->n * sizeof(Ctrl), cudaMemcpyDeviceToHost, b->stream));
+    B_CUDA(cudaStreamSynchronize(b->stream));
+    running = count_unfinished(b);
+    if (running > 0 && total_steps(b) == steps_before)  // would repeat forever
+      return bfail(HF_ERR_TIMEOUT, "ensemble made no progress: no scenario took a step");
+  }
+  if (n_unfinished) *n_unfinished = running;
+  return HF_OK;
+}
+
+int hf_batch_scenario_info(const hf_batch* b, int64_t k, double* t, uint64_t* steps, int* status) {
+  if (!b || k < 0 || k >= b->n) return bfail(HF_ERR_INVALID_ARG, "bad scenario index");
+  const Ctrl& c = b->h_ctrl[k];
+  if (t) *t = c.t;
+  if (steps) *steps = (uint64_t)c.steps;
+  if (status) *status = c.status;
+  return HF_OK;
+}
+
+int hf_batch_get_state(hf_batch* b, int64_t k, double* h, double* hu, double* hv) {
+  if (!b || k < 0 || k >= b->n || !h || !hu || !hv)
+    return bfail(HF_ERR_INVALID_ARG, "bad arguments");
+  Guard guard(b->device);
+  const size_t bytes = (size_t)(b->nr[k] * b->nc[k]) * sizeof(double);
+  const int64_t o = b->off[k];
+  B_CUDA(cudaMemcpyAsync(h, b->h + o, bytes, cudaMemcpyDeviceToHost, b->stream));
+  B_CUDA(cudaMemcpyAsync(hu, b->hu + o, bytes, cudaMemcpyDeviceToHost, b->stream));
+  B_CUDA(cudaMemcpyAsync(hv, b->hv + o, bytes, cudaMemcpyDeviceToHost, b->stream));
+  B_CUDA(cudaStreamSynchronize(b->stream));
+  return HF_OK;
+}
+
+}  // extern "C"

@@ -3,6 +3,8 @@
 
 #include <cstdint>
 
+#include "../../include/hydroflux_gpu.h"
+
 namespace hf {
 
 // Tile geometry of the fused stage kernel: a CTA advances a TX x TY block of
@@ -88,6 +90,8 @@ struct ForcingDev {
 struct StageArgs {
   int nr, nc;
   int tiles_x, tiles_y;
+  int tile_base;  // first tile of this grid in an ensemble's tile list (0 alone)
+  int pad_;
   double dx, dy;
   const double* z;
   const double* n;
@@ -132,5 +136,41 @@ size_t stage_smem_bytes();
 
 // Sets the calling thread's hf_last_error() message and returns `code`.
 int record_error(int code, const char* msg);
+// Shape, SimulationConfig (sim.rs:130-165) and boundary checks of one grid.
+int check_grid_config(const hf_config* cfg, int64_t nr, int64_t nc);
+BcDev boundaries_dev(const hf_boundaries& b);
+
+// Device copies of one grid's forcing tables (host-side owner).
+struct ForcingHost {
+  int n_rain = 0, n_src = 0;
+  double* d_rain_t = nullptr;
+  double* d_rain_v = nullptr;
+  int* d_row = nullptr;
+  int* d_col = nullptr;
+  int* d_off = nullptr;
+  double* d_st = nullptr;
+  double* d_sq = nullptr;
+  int* d_tile_start = nullptr;
+  int* d_tile_order = nullptr;
+  double* d_dh = nullptr;
+  void release_rain();
+  void release_src();
+  ForcingDev dev() const;
+};
+// Validate and upload a rain series / point-source series (see
+// hf_sim_set_rain / hf_sim_set_point_sources); sources are bucketed by tile.
+int forcing_set_rain(ForcingHost& f, int64_t n_points, const double* t, const double* rate);
+int forcing_set_sources(ForcingHost& f, int64_t nr, int64_t nc, int tiles_x, int tiles_y,
+                        int64_t n_sources, const int64_t* rows, const int64_t* cols,
+                        const int64_t* offsets, const double* t, const double* q);
+
+// Ensemble launchers (hf_kernels.cu): args1/args2 are per-scenario device
+// arrays of stage-1 / stage-2 arguments, ctrls the per-scenario control blocks.
+int launch_stage_batch(const StageArgs* args, const int* tile_scn, int total_tiles, int grid,
+                       void* stream);
+int launch_cfl_batch(const StageArgs* args, const int* tile_scn, int total_tiles, int grid,
+                     void* stream);
+int launch_batch_control(Ctrl* ctrls, const StageArgs* args, int n, void* stream);
+int launch_batch_commit(Ctrl* ctrls, int n, void* stream);
 
 }  // namespace hf

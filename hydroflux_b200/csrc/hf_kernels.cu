@@ -83,6 +83,7 @@ __device__ void block_reduce_speeds(double sx, double sy, unsigned long long non
     atomicMax(&c->sy_bits, (unsigned long long)__double_as_longlong(sy));
     if (nonfin) atomicAdd(&c->nonfinite, nonfin);
   }
+  __syncthreads();  // wx/wy/wn may be written again by the next call
 }
 
 // Final state of a cell for the next step: friction (source.rs:130-165),
@@ -136,12 +137,12 @@ __device__ __forceinline__ void commit_clock(Ctrl* c) {
 
 }  // namespace
 
-// One forward-Euler stage (update.rs:805-1211) over a persistent tile loop.
-__global__ void __launch_bounds__(NTHREADS, HF_MIN_BLOCKS) k_stage(const StageArgs A) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  StageSmem& S = *reinterpret_cast<StageSmem*>(smem_raw);
+// One forward-Euler stage (update.rs:805-1211) on one tile of one grid. Called
+// by every thread of the CTA; accumulates the CTA's CFL maxima for the
+// finalize epilogue into (sxm, sym, nonfin).
+__device__ __forceinline__ void stage_tile(const StageArgs& A, StageSmem& S, int tile,
+                                           double& sxm, double& sym, unsigned long long& nonfin) {
   Ctrl* ctrl = A.ctrl;
-  if (!ctrl->active) return;
   const double dt = ctrl->dt;
   const int nr = A.nr, nc = A.nc;
   const double dx = A.dx, dy = A.dy;
@@ -149,11 +150,7 @@ __global__ void __launch_bounds__(NTHREADS, HF_MIN_BLOCKS) k_stage(const StageAr
   const double dt_dy = dt / dy;
   const double half_dx = 0.5 * dx, half_dy = 0.5 * dy;
   const int tid = threadIdx.x;
-  const int ntiles = A.tiles_x * A.tiles_y;
-  double sxm = 0.0, sym = 0.0;
-  unsigned long long nonfin = 0;
-
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+  {
     const int tyi = tile / A.tiles_x;
     const int gi0 = tyi * TY, gj0 = (tile - tyi * A.tiles_x) * TX;
 
@@ -466,9 +463,42 @@ __global__ void __launch_bounds__(NTHREADS, HF_MIN_BLOCKS) k_stage(const StageAr
     }
     __syncthreads();
   }
+}
+
+// One stage of one grid over a persistent tile loop.
+__global__ void __launch_bounds__(NTHREADS, HF_MIN_BLOCKS) k_stage(const StageArgs A) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  StageSmem& S = *reinterpret_cast<StageSmem*>(smem_raw);
+  if (!A.ctrl->active) return;
+  const int ntiles = A.tiles_x * A.tiles_y;
+  double sxm = 0.0, sym = 0.0;
+  unsigned long long nonfin = 0;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
+    stage_tile(A, S, tile, sxm, sym, nonfin);
   if (A.finalize) {
-    block_reduce_speeds(sxm, sym, nonfin, ctrl);
-    if (blockIdx.x == 0 && tid == 0) commit_clock(ctrl);
+    block_reduce_speeds(sxm, sym, nonfin, A.ctrl);
+    if (blockIdx.x == 0 && threadIdx.x == 0) commit_clock(A.ctrl);
+  }
+}
+
+// One stage of every grid of an ensemble in one launch: the persistent grid
+// walks the concatenated tile list of all scenarios; tile t belongs to
+// scenario tile_scn[t], whose arguments (own sizes, dt, forcings, control
+// block) are args[tile_scn[t]]. Finished scenarios' tiles are skipped. The
+// CFL maxima are reduced per tile into the tile's scenario; each scenario's
+// clock is committed afterwards by k_batch_commit.
+__global__ void __launch_bounds__(NTHREADS, HF_MIN_BLOCKS)
+    k_stage_batch(const StageArgs* __restrict__ args, const int* __restrict__ tile_scn,
+                  int total_tiles) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  StageSmem& S = *reinterpret_cast<StageSmem*>(smem_raw);
+  for (int t = blockIdx.x; t < total_tiles; t += gridDim.x) {
+    const StageArgs& A = args[tile_scn[t]];
+    if (!A.ctrl->active) continue;  // uniform over the CTA
+    double sxm = 0.0, sym = 0.0;
+    unsigned long long nonfin = 0;
+    stage_tile(A, S, t - A.tile_base, sxm, sym, nonfin);
+    if (A.finalize) block_reduce_speeds(sxm, sym, nonfin, A.ctrl);
   }
 }
 
@@ -531,11 +561,11 @@ __global__ void __launch_bounds__(NTHREADS) k_cfl(const StageArgs A, int with_gh
   if (blockIdx.x == 0 && threadIdx.x == 0) ctrl->cfl_valid = 1;
 }
 
-// Step control (sim.rs:204-215, 231-245): dt = min(cfl / (sx/dx + sy/dy),
-// max_dt, cap), validity, forcing values at t_new.
-__global__ void k_control(Ctrl* c, double dx, double dy, ForcingDev f) {
-  __shared__ int s_go;
-  if (threadIdx.x == 0) {
+// Step control of one grid (sim.rs:204-215, 231-245): dt = min(cfl /
+// (sx/dx + sy/dy), max_dt, cap), validity, rain at t_new. Returns whether the
+// step runs (also stored in c->active).
+__device__ int control_step(Ctrl* c, double dx, double dy, const ForcingDev& f) {
+  {
     int go = 0;
     if (c->status == 0) {
       go = 1;
@@ -589,17 +619,61 @@ __global__ void k_control(Ctrl* c, double dx, double dy, ForcingDev f) {
       }
     }
     c->active = go;
-    s_go = go;
+    return go;
   }
+}
+
+// Point-source depth increments Q_k(t_new) * dt / (dx * dy) (source.rs:58-60).
+__device__ __forceinline__ void source_increment(const Ctrl* c, double dx, double dy,
+                                                 const ForcingDev& f, int k) {
+  const int a = f.src_off[k], b = f.src_off[k + 1];
+  const double q = series_eval(f.src_t + a, f.src_q + a, b - a, c->t_new);
+  f.src_dh[k] = q * c->dt / (dx * dy);
+}
+
+__global__ void k_control(Ctrl* c, double dx, double dy, ForcingDev f) {
+  __shared__ int s_go;
+  if (threadIdx.x == 0) s_go = control_step(c, dx, dy, f);
   __syncthreads();
-  if (s_go && f.n_src > 0) {
-    const double t_new = c->t_new, dt = c->dt;
-    const double area = dx * dy;
-    for (int k = threadIdx.x; k < f.n_src; k += blockDim.x) {
-      const int a = f.src_off[k], b = f.src_off[k + 1];
-      const double q = series_eval(f.src_t + a, f.src_q + a, b - a, t_new);
-      f.src_dh[k] = q * dt / area;
+  if (s_go)
+    for (int k = threadIdx.x; k < f.n_src; k += blockDim.x) source_increment(c, dx, dy, f, k);
+}
+
+// Per-scenario control of an ensemble: one thread per scenario.
+__global__ void k_batch_control(Ctrl* ctrls, const StageArgs* __restrict__ args, int n) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const StageArgs& A = args[s];
+  if (control_step(&ctrls[s], A.dx, A.dy, A.f))
+    for (int k = 0; k < A.f.n_src; ++k) source_increment(&ctrls[s], A.dx, A.dy, A.f, k);
+}
+
+// Per-scenario clock commit after the ensemble's last stage.
+__global__ void k_batch_commit(Ctrl* ctrls, int n) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < n && ctrls[s].active) commit_clock(&ctrls[s]);
+}
+
+// Ensemble CFL reduction (with ghosts), reduced per tile into its scenario.
+__global__ void __launch_bounds__(NTHREADS)
+    k_cfl_batch(const StageArgs* __restrict__ args, const int* __restrict__ tile_scn,
+                int total_tiles) {
+  for (int t = blockIdx.x; t < total_tiles; t += gridDim.x) {
+    const StageArgs& A = args[tile_scn[t]];
+    const int tile = t - A.tile_base;
+    const int tyi = tile / A.tiles_x;
+    const int gi0 = tyi * TY, gj0 = (tile - tyi * A.tiles_x) * TX;
+    double sxm = 0.0, sym = 0.0;
+    unsigned long long nonfin = 0;
+    for (int q = 0; q < CELLS_PER_THREAD; ++q) {
+      const int gi = gi0 + threadIdx.x / TX + ROWS_PER_PASS * q, gj = gj0 + threadIdx.x % TX;
+      if (gi >= A.nr || gj >= A.nc) continue;
+      const int64_t g = (int64_t)gi * A.nc + gj;
+      const double h = A.in_h[g], hu = A.in_hu[g], hv = A.in_hv[g];
+      cfl_cell(A, gi, gj, g, h, hu, hv, sxm, sym);
+      if (!isfinite(h)) ++nonfin;
     }
+    block_reduce_speeds(sxm, sym, nonfin, A.ctrl);
   }
 }
 
@@ -734,6 +808,8 @@ int stage_grid_size(int tiles, int device) {
     DevGuard dg(device);
     cudaFuncSetAttribute(k_stage, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)sizeof(StageSmem));
+    cudaFuncSetAttribute(k_stage_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(StageSmem));
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stage, NTHREADS, sizeof(StageSmem));
     if (per_sm < 1) per_sm = 1;
     if (device >= 0 && device < 64) cached[device] = per_sm;
@@ -753,6 +829,29 @@ int launch_stage(const StageArgs& a, int grid, void* stream) {
 
 int launch_finalize(const StageArgs& a, int grid, void* stream) {
   k_finalize<<<grid, NTHREADS, 0, (cudaStream_t)stream>>>(a);
+  return cuda_rc(cudaGetLastError());
+}
+
+int launch_stage_batch(const StageArgs* args, const int* tile_scn, int total_tiles, int grid,
+                       void* stream) {
+  k_stage_batch<<<grid, NTHREADS, sizeof(StageSmem), (cudaStream_t)stream>>>(args, tile_scn,
+                                                                             total_tiles);
+  return cuda_rc(cudaGetLastError());
+}
+
+int launch_cfl_batch(const StageArgs* args, const int* tile_scn, int total_tiles, int grid,
+                     void* stream) {
+  k_cfl_batch<<<grid, NTHREADS, 0, (cudaStream_t)stream>>>(args, tile_scn, total_tiles);
+  return cuda_rc(cudaGetLastError());
+}
+
+int launch_batch_control(Ctrl* ctrls, const StageArgs* args, int n, void* stream) {
+  k_batch_control<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(ctrls, args, n);
+  return cuda_rc(cudaGetLastError());
+}
+
+int launch_batch_commit(Ctrl* ctrls, int n, void* stream) {
+  k_batch_commit<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(ctrls, n);
   return cuda_rc(cudaGetLastError());
 }
 

@@ -174,6 +174,51 @@ int hf_sim_set_point_sources(hf_sim* sim, int64_t n_sources, const int64_t* rows
                              const double* q);
 
 /* ---------------------------------------------------------------------------
+ * Ensembles: many independent scenarios (different grid sizes, beds,
+ * roughness, forcings and horizons) advanced together. No counterpart in the
+ * reference, whose callers run one `Simulation` per scenario. Every scenario
+ * keeps run_until semantics (sim.rs:231-245) with its own CFL dt, clock,
+ * step budget and errors; one batch step advances every unfinished scenario
+ * by one of its own steps in a single persistent launch per stage (the tiles
+ * of all scenarios in one list), replayed from CUDA graphs. Results are
+ * bit-identical to solving each scenario alone with hf_sim_*.
+ * Supports the SSP-RK2 integrator (HF_ERR_UNSUPPORTED otherwise).
+ * ------------------------------------------------------------------------- */
+typedef struct hf_batch hf_batch;
+
+typedef struct hf_scenario_desc {
+  hf_mesh_desc mesh;           /* host arrays */
+  const double* h;             /* host SoA initial state */
+  const double* hu;
+  const double* hv;
+  hf_config cfg;
+  double t_end;                /* horizon: the scenario runs until t >= t_end */
+  int64_t n_rain;              /* rain series (see hf_sim_set_rain) */
+  const double* rain_t;
+  const double* rain_rate;
+  int64_t n_sources;           /* point sources (see hf_sim_set_point_sources) */
+  const int64_t* src_rows;
+  const int64_t* src_cols;
+  const int64_t* src_offsets;
+  const double* src_t;
+  const double* src_q;
+} hf_scenario_desc;
+
+int hf_batch_create(int64_t n_scenarios, const hf_scenario_desc* scenarios, int device,
+                    hf_batch** out);
+int hf_batch_destroy(hf_batch* batch);
+/* Up to max_batch_steps batch steps; stops early when every scenario has
+ * reached its horizon or failed. n_unfinished (optional) receives the count
+ * still running. A scenario's failure (DegenerateDt, budget) stops only it:
+ * read it with hf_batch_scenario_info. */
+int hf_batch_run(hf_batch* batch, uint64_t max_batch_steps, int64_t* n_unfinished);
+/* Clock, step count and status (0 or an hf_status_code) of scenario k. */
+int hf_batch_scenario_info(const hf_batch* batch, int64_t k, double* t, uint64_t* steps,
+                           int* status);
+/* Host copy of scenario k's state. */
+int hf_batch_get_state(hf_batch* batch, int64_t k, double* h, double* hu, double* hv);
+
+/* ---------------------------------------------------------------------------
  * Low-level entry points on caller-owned device buffers, mirroring the
  * reference's free functions. All run on `stream` and are asynchronous
  * unless they return a host value (hf_cfl_time_step synchronizes it).
