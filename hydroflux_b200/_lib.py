@@ -53,6 +53,14 @@ PROTOTYPES = {
     "hf_batch_scenario_info": (C.c_int, [_VP, C.c_int64, _D, C.POINTER(C.c_uint64),
                                          C.POINTER(C.c_int)]),
     "hf_batch_get_state": (C.c_int, [_VP, C.c_int64, _VP, _VP, _VP]),
+    "hf_server_create": (C.c_int, [C.c_int, C.c_uint64, C.c_int, C.POINTER(_VP)]),
+    "hf_server_destroy": (C.c_int, [_VP]),
+    "hf_server_admit": (C.c_int, [_VP, C.POINTER(abi.hf_scenario_desc), C.POINTER(C.c_int)]),
+    "hf_server_advance": (C.c_int, [_VP, C.c_uint64, C.POINTER(C.c_int)]),
+    "hf_server_finished": (C.c_int, [_VP, C.POINTER(C.c_int), C.c_int, C.POINTER(C.c_int)]),
+    "hf_server_collect": (C.c_int, [_VP, C.c_int, _VP, _VP, _VP, _D, C.POINTER(C.c_uint64),
+                                    C.POINTER(C.c_int)]),
+    "hf_server_usage": (C.c_int, [_VP, C.POINTER(C.c_uint64), C.POINTER(C.c_int)]),
     "hf_workspace_create": (C.c_int, [C.c_int64, C.c_int64, C.c_int, C.POINTER(_VP)]),
     "hf_workspace_destroy": (C.c_int, [_VP]),
     "hf_cfl_time_step": (C.c_int, [C.POINTER(abi.hf_grid), _VP, _VP, _VP,

@@ -19,6 +19,7 @@ HF_ERR_CUDA = -7
 HF_ERR_INVALID_ARG = -8
 HF_ERR_OUT_OF_MEMORY = -9
 HF_ERR_UNSUPPORTED = -10
+HF_ERR_CAPACITY = -11
 
 HF_BC_TRANSMISSIVE = 0
 HF_BC_WALL = 1

@@ -75,6 +75,7 @@ struct hf_batch {
   StageArgs* d_args1 = nullptr;
   StageArgs* d_args2 = nullptr;
   int* d_tile_scn = nullptr;
+  int* d_n_tiles = nullptr;  // device copy of total_tiles (read by the stage kernel)
   std::vector<ForcingHost> forcing;
   std::vector<int64_t> off, nr, nc;
   std::vector<double> t_end;
@@ -94,7 +95,7 @@ void destroy_batch(hf_batch* b) {
     f.release_src();
   }
   for (void* p : {(void*)b->buf, (void*)b->d_ctrl, (void*)b->d_args1, (void*)b->d_args2,
-                  (void*)b->d_tile_scn})
+                  (void*)b->d_tile_scn, (void*)b->d_n_tiles})
     if (p) cudaFree(p);
   if (b->h_ctrl) cudaFreeHost(b->h_ctrl);
   if (b->stream) cudaStreamDestroy(b->stream);
@@ -103,9 +104,9 @@ void destroy_batch(hf_batch* b) {
 
 int enqueue_batch_step(hf_batch* b) {
   if (launch_batch_control(b->d_ctrl, b->d_args1, b->n, b->stream)) return bcuda(cudaGetLastError(), "control");
-  if (launch_stage_batch(b->d_args1, b->d_tile_scn, b->total_tiles, b->grid, b->stream))
+  if (launch_stage_batch(b->d_args1, b->d_tile_scn, b->d_n_tiles, b->grid, b->stream))
     return bcuda(cudaGetLastError(), "stage 1");
-  if (launch_stage_batch(b->d_args2, b->d_tile_scn, b->total_tiles, b->grid, b->stream))
+  if (launch_stage_batch(b->d_args2, b->d_tile_scn, b->d_n_tiles, b->grid, b->stream))
     return bcuda(cudaGetLastError(), "stage 2");
   if (launch_batch_commit(b->d_ctrl, b->n, b->stream)) return bcuda(cudaGetLastError(), "commit");
   return HF_OK;
@@ -199,6 +200,7 @@ int hf_batch_create(int64_t n_scenarios, const hf_scenario_desc* sc, int device,
       cudaMalloc((void**)&b->d_args1, b->n * sizeof(StageArgs)) != cudaSuccess ||
       cudaMalloc((void**)&b->d_args2, b->n * sizeof(StageArgs)) != cudaSuccess ||
       cudaMalloc((void**)&b->d_tile_scn, b->total_tiles * sizeof(int)) != cudaSuccess ||
+      cudaMalloc((void**)&b->d_n_tiles, sizeof(int)) != cudaSuccess ||
       cudaMallocHost((void**)&b->h_ctrl, b->n * sizeof(Ctrl)) != cudaSuccess)
     return done(bcuda(cudaGetLastError(), "cudaMalloc(ensemble tables)"));
   std::vector<StageArgs> a1(b->n), a2(b->n);
@@ -272,10 +274,11 @@ int hf_batch_create(int64_t n_scenarios, const hf_scenario_desc* sc, int device,
   if (cudaMemcpy(b->d_args1, a1.data(), b->n * sizeof(StageArgs), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(b->d_args2, a2.data(), b->n * sizeof(StageArgs), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(b->d_tile_scn, tile_scn.data(), b->total_tiles * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(b->d_n_tiles, &b->total_tiles, sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(b->d_ctrl, b->h_ctrl, b->n * sizeof(Ctrl), cudaMemcpyHostToDevice) != cudaSuccess)
     return done(bcuda(cudaGetLastError(), "upload ensemble tables"));
   // CFL accumulators of every scenario from its initial state (with ghosts).
-  if (launch_cfl_batch(b->d_args1, b->d_tile_scn, b->total_tiles, b->grid, b->stream))
+  if (launch_cfl_batch(b->d_args1, b->d_tile_scn, 0, b->total_tiles, b->grid, b->stream))
     return done(bcuda(cudaGetLastError(), "initial CFL"));
   if (cudaStreamSynchronize(b->stream) != cudaSuccess)
     return done(bcuda(cudaGetLastError(), "initial CFL"));

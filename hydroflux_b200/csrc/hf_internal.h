@@ -166,10 +166,12 @@ int forcing_set_sources(ForcingHost& f, int64_t nr, int64_t nc, int tiles_x, int
 
 // Ensemble launchers (hf_kernels.cu): args1/args2 are per-scenario device
 // arrays of stage-1 / stage-2 arguments, ctrls the per-scenario control blocks.
-int launch_stage_batch(const StageArgs* args, const int* tile_scn, int total_tiles, int grid,
+// n_tiles is a device int (the tile list length, read at launch time); the
+// CFL reduction covers tiles [first_tile, last_tile).
+int launch_stage_batch(const StageArgs* args, const int* tile_scn, const int* n_tiles, int grid,
                        void* stream);
-int launch_cfl_batch(const StageArgs* args, const int* tile_scn, int total_tiles, int grid,
-                     void* stream);
+int launch_cfl_batch(const StageArgs* args, const int* tile_scn, int first_tile, int last_tile,
+                     int grid, void* stream);
 int launch_batch_control(Ctrl* ctrls, const StageArgs* args, int n, void* stream);
 int launch_batch_commit(Ctrl* ctrls, int n, void* stream);
 

@@ -489,9 +489,10 @@ __global__ void __launch_bounds__(NTHREADS, HF_MIN_BLOCKS) k_stage(const StageAr
 // clock is committed afterwards by k_batch_commit.
 __global__ void __launch_bounds__(NTHREADS, HF_MIN_BLOCKS)
     k_stage_batch(const StageArgs* __restrict__ args, const int* __restrict__ tile_scn,
-                  int total_tiles) {
+                  const int* __restrict__ n_tiles) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   StageSmem& S = *reinterpret_cast<StageSmem*>(smem_raw);
+  const int total_tiles = *n_tiles;  // device-resident: a graph serves any set of scenarios
   for (int t = blockIdx.x; t < total_tiles; t += gridDim.x) {
     const StageArgs& A = args[tile_scn[t]];
     if (!A.ctrl->active) continue;  // uniform over the CTA
@@ -657,8 +658,8 @@ __global__ void k_batch_commit(Ctrl* ctrls, int n) {
 // Ensemble CFL reduction (with ghosts), reduced per tile into its scenario.
 __global__ void __launch_bounds__(NTHREADS)
     k_cfl_batch(const StageArgs* __restrict__ args, const int* __restrict__ tile_scn,
-                int total_tiles) {
-  for (int t = blockIdx.x; t < total_tiles; t += gridDim.x) {
+                int first_tile, int last_tile) {
+  for (int t = first_tile + blockIdx.x; t < last_tile; t += gridDim.x) {
     const StageArgs& A = args[tile_scn[t]];
     const int tile = t - A.tile_base;
     const int tyi = tile / A.tiles_x;
@@ -832,16 +833,17 @@ int launch_finalize(const StageArgs& a, int grid, void* stream) {
   return cuda_rc(cudaGetLastError());
 }
 
-int launch_stage_batch(const StageArgs* args, const int* tile_scn, int total_tiles, int grid,
+int launch_stage_batch(const StageArgs* args, const int* tile_scn, const int* n_tiles, int grid,
                        void* stream) {
   k_stage_batch<<<grid, NTHREADS, sizeof(StageSmem), (cudaStream_t)stream>>>(args, tile_scn,
-                                                                             total_tiles);
+                                                                             n_tiles);
   return cuda_rc(cudaGetLastError());
 }
 
-int launch_cfl_batch(const StageArgs* args, const int* tile_scn, int total_tiles, int grid,
-                     void* stream) {
-  k_cfl_batch<<<grid, NTHREADS, 0, (cudaStream_t)stream>>>(args, tile_scn, total_tiles);
+int launch_cfl_batch(const StageArgs* args, const int* tile_scn, int first_tile, int last_tile,
+                     int grid, void* stream) {
+  if (last_tile <= first_tile) return 0;
+  k_cfl_batch<<<grid, NTHREADS, 0, (cudaStream_t)stream>>>(args, tile_scn, first_tile, last_tile);
   return cuda_rc(cudaGetLastError());
 }
 

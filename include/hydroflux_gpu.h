@@ -45,7 +45,8 @@ enum hf_status_code {
   HF_ERR_CUDA = -7,           /* CUDA runtime failure */
   HF_ERR_INVALID_ARG = -8,    /* bad pointer / index; the reference panics here */
   HF_ERR_OUT_OF_MEMORY = -9,  /* device allocation failed */
-  HF_ERR_UNSUPPORTED = -10    /* feature not available for this configuration */
+  HF_ERR_UNSUPPORTED = -10,   /* feature not available for this configuration */
+  HF_ERR_CAPACITY = -11       /* server: no free slot or over the HBM budget (retry later) */
 };
 
 /* Boundary kinds (solver-2d/src/boundary.rs:80-104). */
@@ -217,6 +218,35 @@ int hf_batch_scenario_info(const hf_batch* batch, int64_t k, double* t, uint64_t
                            int* status);
 /* Host copy of scenario k's state. */
 int hf_batch_get_state(hf_batch* batch, int64_t k, double* h, double* hu, double* hv);
+
+/* ---------------------------------------------------------------------------
+ * Serving: continuous batching of flood scenarios on one GPU. No counterpart
+ * in the reference. Scenarios are admitted into slots while a slot is free
+ * and their fields (64 B per cell) fit the HBM budget, stay resident on the
+ * device between steps, and advance together with every other admitted
+ * scenario (one persistent launch per stage over all their tiles, one
+ * captured CUDA graph for any mix). A scenario finishes at its horizon (or on
+ * its own error) and is collected, which frees its slot and memory for the
+ * next request. Each scenario's result is bit-identical to solving it alone.
+ * ------------------------------------------------------------------------- */
+typedef struct hf_server hf_server;
+
+int hf_server_create(int device, uint64_t hbm_budget_bytes, int max_slots, hf_server** out);
+int hf_server_destroy(hf_server* server);
+/* Copies the scenario to the device and admits it (*slot receives its id), or
+ * returns HF_ERR_CAPACITY when no slot is free or it would exceed the budget. */
+int hf_server_admit(hf_server* server, const hf_scenario_desc* scenario, int* slot);
+/* Up to n_batch_steps batch steps over the admitted scenarios; returns early
+ * once some scenario finishes. n_finished receives the count awaiting
+ * collection. */
+int hf_server_advance(hf_server* server, uint64_t n_batch_steps, int* n_finished);
+/* Ids of finished, uncollected slots (up to cap). */
+int hf_server_finished(hf_server* server, int* slots, int cap, int* n);
+/* Result of a finished slot (state may be NULL to skip it), then frees it. */
+int hf_server_collect(hf_server* server, int slot, double* h, double* hu, double* hv, double* t,
+                      uint64_t* steps, int* status);
+/* Bytes of the budget in use and occupied slots. */
+int hf_server_usage(const hf_server* server, uint64_t* bytes_in_use, int* occupied);
 
 /* ---------------------------------------------------------------------------
  * Low-level entry points on caller-owned device buffers, mirroring the
