@@ -61,6 +61,15 @@ PROTOTYPES = {
     "hf_server_collect": (C.c_int, [_VP, C.c_int, _VP, _VP, _VP, _D, C.POINTER(C.c_uint64),
                                     C.POINTER(C.c_int)]),
     "hf_server_usage": (C.c_int, [_VP, C.POINTER(C.c_uint64), C.POINTER(C.c_int)]),
+    "hf_calib_create": (C.c_int, [C.POINTER(abi.hf_scenario_desc), C.c_int64, C.c_int64, _I64P,
+                                  C.c_int64, C.c_int, C.POINTER(_VP)]),
+    "hf_calib_destroy": (C.c_int, [_VP]),
+    "hf_calib_set_observations": (C.c_int, [_VP, _D]),
+    "hf_calib_run": (C.c_int, [_VP, _D, C.c_int, _D, _D, C.POINTER(C.c_int64)]),
+    "hf_tangent": (C.c_int, [_VP, _D, _D, _D, _D, _D, _D, _D]),
+    "hf_grad_manning": (C.c_int, [_VP, _D, _D, _D, _D, _D, _D]),
+    "hf_calib_final_state": (C.c_int, [_VP, _D, _D, _D, _D, _D, _D]),
+    "hf_calib_dt": (C.c_int, [_VP, _D, C.POINTER(C.c_int64)]),
     "hf_workspace_create": (C.c_int, [C.c_int64, C.c_int64, C.c_int, C.POINTER(_VP)]),
     "hf_workspace_destroy": (C.c_int, [_VP]),
     "hf_cfl_time_step": (C.c_int, [C.POINTER(abi.hf_grid), _VP, _VP, _VP,

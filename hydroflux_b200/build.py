@@ -17,7 +17,8 @@ ROOT = os.path.dirname(HERE)
 INCLUDE = os.path.join(ROOT, "include")
 OUT = os.path.join(HERE, "libhydroflux_gpu.so")
 
-SOURCES = ["hf_kernels.cu", "hf_api.cu", "hf_noalloc.cu", "hf_batch.cu", "hf_serve.cu"]
+SOURCES = ["hf_kernels.cu", "hf_api.cu", "hf_noalloc.cu", "hf_batch.cu", "hf_serve.cu",
+           "hf_adjoint.cu", "hf_calib.cu"]
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-prec-div=true",
               "-prec-sqrt=true", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",

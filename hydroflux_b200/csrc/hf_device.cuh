@@ -4,6 +4,11 @@
 // (franciscoparrao/hydroflux, solver-2d) so that, compiled with
 // --fmad=false and IEEE division / square root, it rounds like the
 // reference's f64 code. Citations are file:line in that crate.
+//
+// The state arithmetic is generic over the scalar T (hf_scalar.cuh): double
+// for the production step, DualD for the forward-mode tangent, like the
+// reference's `T: Real` code. Bed elevations are never differentiated and
+// stay double; branches read values only.
 #pragma once
 
 #include <cstdint>
@@ -11,6 +16,7 @@
 #include "hf_arith.h"
 #include "hf_internal.h"
 #include "hf_pow.h"
+#include "hf_scalar.cuh"
 
 namespace hf {
 
@@ -25,40 +31,47 @@ constexpr double DRY_INFLOW_H_MAX = 10.0;
 enum { BC_TRANSMISSIVE = 0, BC_WALL = 1, BC_DISCHARGE = 2, BC_DEPTH = 3 };
 enum { SIDE_NORTH = 0, SIDE_SOUTH = 1, SIDE_WEST = 2, SIDE_EAST = 3 };
 
-struct Ghost {
-  double h, hu, hv, z;
+template <class T> struct GhostT {
+  T h, hu, hv;
+  double z;
 };
+using Ghost = GhostT<double>;
 
 // ghost_cell (boundary.rs:193-219) with ghost_state (274-333) and ghost_bed
 // (335-367). `c0` is the boundary cell, `c1` the next cell inward along the
-// face normal (only read for Discharge / Depth, which need two cells).
-__device__ __forceinline__ Ghost ghost_cell(int side, const BcDev& bc, double h, double hu,
-                                            double hv, const double* __restrict__ z,
-                                            const double* __restrict__ nman, int64_t c0,
-                                            int64_t c1, double d_normal) {
+// face normal (only read for Discharge / Depth, which need two cells). The
+// Manning value (and, for DualD, its tangent `dnman`) is read only by the
+// dry-inflow Discharge ghost.
+template <class T>
+__device__ __forceinline__ GhostT<T> ghost_cell(int side, const BcDev& bc, T h, T hu, T hv,
+                                                const double* __restrict__ z,
+                                                const double* __restrict__ nman,
+                                                const double* __restrict__ dnman, int64_t c0,
+                                                int64_t c1, double d_normal) {
   const int kind = bc.kind[side];
-  const double val = bc.val[side];
+  const double bval = bc.val[side];
   const bool xf = side >= SIDE_WEST;
-  Ghost g{h, hu, hv, 0.0};
+  GhostT<T> g{h, hu, hv, 0.0};
   if (kind == BC_WALL) {
     if (xf) g.hu = -hu; else g.hv = -hv;
   } else if (kind == BC_DISCHARGE) {
-    if (xf) g.hu = val; else g.hv = val;
+    if (xf) g.hu = cst<T>(bval); else g.hv = cst<T>(bval);
   } else if (kind == BC_DEPTH) {
-    g.h = val;
+    g.h = cst<T>(bval);
   }
   if (kind == BC_TRANSMISSIVE || kind == BC_WALL) {
     g.z = z[c0];
   } else {
     g.z = z[c0] * 2.0 - z[c1];
   }
-  if (kind == BC_DISCHARGE && h < H_DRY) {
+  if (kind == BC_DISCHARGE && val(h) < H_DRY) {
     // |bed_slope| along the normal (boundary.rs:241-271); |a-b| is exact in
     // either order, so the side-specific operand order does not matter.
     const double slope_mag = fabs(hfa::div_rn(z[c0] - z[c1], d_normal));
     if (slope_mag > DRY_INFLOW_SLOPE_THRESHOLD) {
-      const double h_n = hfpow::pow_3_5(nman[c0] * hfa::div_rn(fabs(val), sqrt(slope_mag)));
-      g.h = fmin(h_n, DRY_INFLOW_H_MAX);
+      const T n0 = Field<T>::ld(nman, dnman, c0);
+      const T h_n = r_pow35(n0 * hfa::div_rn(fabs(bval), sqrt(slope_mag)));
+      g.h = r_min(h_n, cst<T>(DRY_INFLOW_H_MAX));
     }
   }
   return g;
@@ -67,23 +80,24 @@ __device__ __forceinline__ Ghost ghost_cell(int side, const BcDev& bc, double h,
 // hllc_normal_flux (riemann.rs:114-204). Only the side that the sampling
 // picks has its tangential velocity and star depth evaluated; those are the
 // only values the reference's result reads, so the result is identical.
-__device__ __forceinline__ void hllc_normal(double h_l, double qn_l, double qt_l, double h_r,
-                                            double qn_r, double qt_r, double& o_m, double& o_n,
-                                            double& o_t) {
-  const bool wl = h_l > DRY_TOL;
-  const bool wr = h_r > DRY_TOL;
+template <class T>
+__device__ __forceinline__ void hllc_normal(T h_l, T qn_l, T qt_l, T h_r, T qn_r, T qt_r,
+                                            T& o_m, T& o_n, T& o_t) {
+  const bool wl = val(h_l) > DRY_TOL;
+  const bool wr = val(h_r) > DRY_TOL;
+  const T Z = cst<T>(0.0);
   if (!wl && !wr) {
-    o_m = 0.0; o_n = 0.0; o_t = 0.0;
+    o_m = Z; o_n = Z; o_t = Z;
     return;
   }
-  const double cl = wl ? sqrt(h_l * GRAVITY) : 0.0;
-  const double cr = wr ? sqrt(h_r * GRAVITY) : 0.0;
-  const double un_l = wl ? hfa::div_rn(qn_l, h_l) : 0.0;
-  const double un_r = wr ? hfa::div_rn(qn_r, h_r) : 0.0;
-  double sl, sr;
+  const T cl = wl ? r_sqrt_pos(h_l * GRAVITY) : Z;
+  const T cr = wr ? r_sqrt_pos(h_r * GRAVITY) : Z;
+  const T un_l = wl ? dv(qn_l, h_l) : Z;
+  const T un_r = wr ? dv(qn_r, h_r) : Z;
+  T sl, sr;
   if (wl && wr) {
-    sl = fmin(un_l - cl, un_r - cr);
-    sr = fmax(un_l + cl, un_r + cr);
+    sl = r_min(un_l - cl, un_r - cr);
+    sr = r_max(un_l + cl, un_r + cr);
   } else if (!wl) {
     sl = un_r - cr * 2.0;
     sr = un_r + cr;
@@ -92,26 +106,26 @@ __device__ __forceinline__ void hllc_normal(double h_l, double qn_l, double qt_l
     sr = un_l + cl * 2.0;
   }
   bool left, star;
-  double s_star = 0.0;
-  if (sl >= 0.0) {
+  T s_star = Z;
+  if (val(sl) >= 0.0) {
     left = true; star = false;
-  } else if (sr <= 0.0) {
+  } else if (val(sr) <= 0.0) {
     left = false; star = false;
   } else {
-    const double denom = h_r * (un_r - sr) - h_l * (un_l - sl);
-    s_star = fabs(denom) > 1.0e-12
-                 ? hfa::div_rn(h_r * (un_r - sr) * sl - h_l * (un_l - sl) * sr, denom)
+    const T denom = h_r * (un_r - sr) - h_l * (un_l - sl);
+    s_star = fabs(val(denom)) > 1.0e-12
+                 ? dv(h_r * (un_r - sr) * sl - h_l * (un_l - sl) * sr, denom)
                  : (sl + sr) * 0.5;
-    left = s_star >= 0.0;
+    left = val(s_star) >= 0.0;
     star = true;
   }
-  const double h = left ? h_l : h_r;
-  const double qn = left ? qn_l : qn_r;
-  const double qt = left ? qt_l : qt_r;
-  const double un = left ? un_l : un_r;
+  const T h = left ? h_l : h_r;
+  const T qn = left ? qn_l : qn_r;
+  const T qt = left ? qt_l : qt_r;
+  const T un = left ? un_l : un_r;
   const bool wet = left ? wl : wr;
-  const double ut = wet ? hfa::div_rn(qt, h) : 0.0;
-  double fm = 0.0, fn = 0.0, ft = 0.0;
+  const T ut = wet ? dv(qt, h) : Z;
+  T fm = Z, fn = Z, ft = Z;
   if (wet) {
     fm = qn;
     fn = qn * un + h * h * (0.5 * GRAVITY);
@@ -121,8 +135,8 @@ __device__ __forceinline__ void hllc_normal(double h_l, double qn_l, double qt_l
     o_m = fm; o_n = fn; o_t = ft;
     return;
   }
-  const double s = left ? sl : sr;
-  const double hs = hfa::div_rn(h * (s - un), s - s_star);
+  const T s = left ? sl : sr;
+  const T hs = dv(h * (s - un), s - s_star);
   o_m = fm + (hs - h) * s;
   o_n = fn + (hs * s_star - qn) * s;
   o_t = ft + (hs * ut - qt) * s;
@@ -133,25 +147,26 @@ __device__ __forceinline__ void hllc_normal(double h_l, double qn_l, double qt_l
 // (h, normal momentum, tangential momentum). Outputs: mass, the normal
 // momentum flux seen by the minus (left/top) and plus (right/bottom) cell,
 // and the tangential momentum flux.
-__device__ __forceinline__ void wb_face(double hL, double qnL, double qtL, double hR, double qnR,
-                                        double qtR, double zf, double& mass, double& n_minus,
-                                        double& n_plus, double& tang) {
+template <class T>
+__device__ __forceinline__ void wb_face(T hL, T qnL, T qtL, T hR, T qnR, T qtR, double zf,
+                                        T& mass, T& n_minus, T& n_plus, T& tang) {
   const double z_max = fmax(zf, zf);
-  const double hsL = fmax(hL + zf - z_max, 0.0);
-  const double hsR = fmax(hR + zf - z_max, 0.0);
-  double unL = 0.0, utL = 0.0, unR = 0.0, utR = 0.0;
-  if (hL > H_VEL) {
-    unL = hfa::div_rn(qnL, hL);
-    utL = hfa::div_rn(qtL, hL);
+  const T Z = cst<T>(0.0);
+  const T hsL = r_max(hL + zf - z_max, Z);
+  const T hsR = r_max(hR + zf - z_max, Z);
+  T unL = Z, utL = Z, unR = Z, utR = Z;
+  if (val(hL) > H_VEL) {
+    unL = dv(qnL, hL);
+    utL = dv(qtL, hL);
   }
-  if (hR > H_VEL) {
-    unR = hfa::div_rn(qnR, hR);
-    utR = hfa::div_rn(qtR, hR);
+  if (val(hR) > H_VEL) {
+    unR = dv(qnR, hR);
+    utR = dv(qtR, hR);
   }
-  double fm, fn, ft;
-  hllc_normal(hsL, hsL * unL, hsL * utL, hsR, hsR * unR, hsR * utR, fm, fn, ft);
-  const double corrL = (hL * hL - hsL * hsL) * (0.5 * GRAVITY);
-  const double corrR = (hR * hR - hsR * hsR) * (0.5 * GRAVITY);
+  T fm, fn, ft;
+  hllc_normal<T>(hsL, hsL * unL, hsL * utL, hsR, hsR * unR, hsR * utR, fm, fn, ft);
+  const T corrL = (hL * hL - hsL * hsL) * (0.5 * GRAVITY);
+  const T corrR = (hR * hR - hsR * hsR) * (0.5 * GRAVITY);
   mass = fm;
   n_minus = fn + corrL;
   n_plus = fn + corrR;
@@ -159,10 +174,10 @@ __device__ __forceinline__ void wb_face(double hL, double qnL, double qtL, doubl
 }
 
 // The reference's minmod(dl / d, dr / d) evaluated literally (update.rs:362-370).
-__device__ __noinline__ double minmod_literal(double dl, double dr, double d) {
-  const double a = hfa::div_rn(dl, d), b = hfa::div_rn(dr, d);
-  if (a * b <= 0.0) return 0.0;
-  return fabs(a) < fabs(b) ? a : b;
+template <class T> __device__ __noinline__ T minmod_literal(T dl, T dr, double d) {
+  const T a = dv(dl, d), b = dv(dr, d);
+  if (val(a) * val(b) <= 0.0) return cst<T>(0.0);
+  return fabs(val(a)) < fabs(val(b)) ? a : b;
 }
 
 // minmod(dl / d, dr / d) with one division. Division by d > 0 keeps the sign
@@ -171,24 +186,39 @@ __device__ __noinline__ double minmod_literal(double dl, double dr, double d) {
 // value). A zero difference makes the reference's product of quotients +-0,
 // hence 0. Tiny or infinite operands, where the reference's product of
 // quotients could underflow or be NaN, take the literal path out of line.
-__device__ __forceinline__ double minmod_div(double dl, double dr, double d) {
-  const bool finite = hfa::is_finite(dl) && hfa::is_finite(dr);
-  if ((hfa::is_zero(dl) || hfa::is_zero(dr)) && finite) return 0.0;
-  if (!finite || fabs(dl) < 1.0e-140 || fabs(dr) < 1.0e-140) return minmod_literal(dl, dr, d);
-  if (dl * dr <= 0.0) return 0.0;
-  return hfa::div_rn(fabs(dl) < fabs(dr) ? dl : dr, d);
+template <class T> __device__ __forceinline__ T minmod_div(T dl, T dr, double d) {
+  const double l = val(dl), r = val(dr);
+  const bool finite = hfa::is_finite(l) && hfa::is_finite(r);
+  if ((hfa::is_zero(l) || hfa::is_zero(r)) && finite) return cst<T>(0.0);
+  if (!finite || fabs(l) < 1.0e-140 || fabs(r) < 1.0e-140) return minmod_literal<T>(dl, dr, d);
+  if (l * r <= 0.0) return cst<T>(0.0);
+  return dv(fabs(l) < fabs(r) ? dl : dr, d);
+}
+
+// Which operand minmod_div(dl, dr, d) returns: -1 for the constant zero, 0
+// for dl / d, 1 for dr / d. Same branches as minmod_div / minmod_literal.
+__device__ __forceinline__ int minmod_pick(double l, double r, double d) {
+  const bool finite = hfa::is_finite(l) && hfa::is_finite(r);
+  if ((hfa::is_zero(l) || hfa::is_zero(r)) && finite) return -1;
+  if (!finite || fabs(l) < 1.0e-140 || fabs(r) < 1.0e-140) {
+    const double a = hfa::div_rn(l, d), b = hfa::div_rn(r, d);
+    if (a * b <= 0.0) return -1;
+    return fabs(a) < fabs(b) ? 0 : 1;
+  }
+  if (l * r <= 0.0) return -1;
+  return fabs(l) < fabs(r) ? 0 : 1;
 }
 
 // Manning friction on one cell (source.rs:150-164); h^(4/3) correctly rounded.
-__device__ __forceinline__ void friction_cell(double h, double& hu, double& hv, double n,
-                                              double dt, double dry_tol) {
-  if (h <= dry_tol) return;
-  if (n == 0.0) return;
+template <class T>
+__device__ __forceinline__ void friction_cell(T h, T& hu, T& hv, T n, double dt, double dry_tol) {
+  if (val(h) <= dry_tol) return;
+  if (val(n) == 0.0) return;
   const double dt_g = dt * GRAVITY;
-  const double speed = hfa::div_rn(hfa::sqrt_rn(hu * hu + hv * hv), h);
-  const double factor = hfa::div_rn(n * n * speed, hfpow::pow_4_3(h)) * dt_g + 1.0;
-  hu = hfa::div_rn(hu, factor);
-  hv = hfa::div_rn(hv, factor);
+  const T speed = dv(r_sqrt(hu * hu + hv * hv), h);
+  const T factor = dv(n * n * speed, r_pow43(h)) * dt_g + 1.0;
+  hu = dv(hu, factor);
+  hv = dv(hv, factor);
 }
 
 // Piecewise-linear series (same definition as the host forcing descriptor).

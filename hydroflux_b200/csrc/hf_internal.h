@@ -38,7 +38,9 @@ struct BcDev {
   double val[4];  // q for Discharge, h for Depth
 };
 
-enum CtrlMode { MODE_FIXED = 0, MODE_STEP = 1, MODE_RUN = 2 };
+// MODE_REPLAY takes step k's dt from replay_dt[k] (a recorded dt sequence)
+// for steps < replay_n.
+enum CtrlMode { MODE_FIXED = 0, MODE_STEP = 1, MODE_RUN = 2, MODE_REPLAY = 3 };
 
 // Device-resident step control block. dt, the simulation clock and the CFL
 // accumulators live here, so a step needs no host round trip.
@@ -67,6 +69,8 @@ struct Ctrl {
   double err_dt;
   double err_t;
   long long err_step;
+  const double* replay_dt;  // MODE_REPLAY
+  long long replay_n;
 };
 
 // Forcing tables on the device (piecewise-linear series). Point sources are
@@ -85,6 +89,22 @@ struct ForcingDev {
   const int* tile_start;
   const int* tile_order;
   double* src_dh;  // per source, set each step by the control kernel
+};
+
+// Tangent arrays of a DualD (forward-mode) stage, parallel to the value
+// arrays of StageArgs; the f64 kernels never read them. A null input
+// tangent is a zero tangent.
+struct TanPtrs {
+  const double* in_h = nullptr;
+  const double* in_hu = nullptr;
+  const double* in_hv = nullptr;
+  double* out_h = nullptr;
+  double* out_hu = nullptr;
+  double* out_hv = nullptr;
+  const double* un_h = nullptr;
+  const double* un_hu = nullptr;
+  const double* un_hv = nullptr;
+  const double* n = nullptr;  // Manning tangent
 };
 
 struct StageArgs {
@@ -110,6 +130,7 @@ struct StageArgs {
   int finalize;  // friction + forcings + CFL reduction + clock commit
   double dry_tol;
   ForcingDev f;
+  TanPtrs tan;   // DualD kernels only
 };
 
 // Launchers (hf_kernels.cu).
@@ -133,6 +154,34 @@ int launch_hllc(int x_dir, int64_t n, const double* ul, const double* ur, double
                 void* stream);
 int stage_grid_size(int tiles, int device);
 size_t stage_smem_bytes();
+// DualD tangent stage / finalize (same arguments; tangent arrays in a.tan).
+int stage_dual_grid_size(int tiles, int device);
+int launch_stage_dual(const StageArgs& a, int grid, void* stream);
+int launch_finalize_dual(const StageArgs& a, int grid, void* stream);
+
+// Adjoint of one stage (hf_adjoint.cu). `a` is the stage's forward arguments
+// (with combine / finalize as run); lam_* the adjoint of its output. Writes
+// halo[tile][4][..] (adjoint of the input h, hu, hv and of n over each tile
+// and its 3-cell halo) and, with a.combine, 0.5 * the combination's adjoint
+// into lam_un_*. Grid from adj_grid_size().
+size_t adj_halo_doubles_per_tile();
+int adj_grid_size(int tiles, int device);
+int launch_stage_adj(const StageArgs& a, const double* lam_h, const double* lam_hu,
+                     const double* lam_hv, double* lam_un_h, double* lam_un_hu,
+                     double* lam_un_hv, double* halo, int grid, void* stream);
+// out = sum of the halo contributions (+ add when non-null); grad_n += the
+// Manning part.
+int launch_adj_gather(int nr, int nc, int tiles_x, int tiles_y, const double* halo,
+                      const double* add_h, const double* add_hu, const double* add_hv,
+                      double* out_h, double* out_hu, double* out_hv, double* grad_n,
+                      void* stream);
+int launch_adj_seed(double* lam_h, const int64_t* cells, int n_gauges, const double* gauge_h,
+                    const double* obs, void* stream);
+int launch_calib_pre(const Ctrl* c, double* dts, double* ts, long long cap, void* stream);
+int launch_calib_post(const Ctrl* c, const double* h, const double* dh, const int64_t* cells,
+                      int n_gauges, double* gauge_h, double* gauge_dh, long long cap,
+                      void* stream);
+int launch_calib_rewind(Ctrl* c, const double* ts, long long k, void* stream);
 
 // Sets the calling thread's hf_last_error() message and returns `code`.
 int record_error(int code, const char* msg);

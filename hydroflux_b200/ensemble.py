@@ -33,7 +33,7 @@ def _ip(a):
 
 def scenario_config(s: Scenario, max_steps: int = 10_000_000) -> abi.hf_config:
     return abi.make_config(cfl=s.cfl, boundaries=abi.make_boundaries(*s.bcs), max_dt=s.max_dt,
-                           max_steps=max_steps)
+                           max_steps=max_steps, integrator=s.integrator)
 
 
 class _Desc:

@@ -9,6 +9,9 @@
   {0.025, 0.035, 0.05, 0.08}, initially dry, one point inflow at the
   upstream thalweg with a triangular hydrograph 0 -> peak at 30 min -> 0 at
   60 min, rain 50 mm/h everywhere, transmissive (open) sides, CFL 0.5.
+* `calibration_problem(n)` -- the valley with a smooth log-normal Manning
+  field (median 0.04, sigma 0.3, 10-cell correlation), 16 thalweg gauges and
+  a hidden Manning field of the same law that makes the observations.
 
 Random numbers come from splitmix64 keyed by (seed, stream, index), so
 every generator is reproducible element by element.
@@ -62,6 +65,7 @@ class Scenario:
     t_end: float = 0.0
     max_dt: float = 60.0
     rain: Optional[Tuple[np.ndarray, np.ndarray]] = None          # (t, rate)
+    integrator: int = 1  # 0 forward Euler, 1 SSP-RK2
     sources: List[Tuple[int, int, np.ndarray, np.ndarray]] = field(default_factory=list)
 
     @property
@@ -137,6 +141,67 @@ def valley(n: int = 4096, dx: float = 5.0, seed: int = 0, peak: float = 500.0,
     rain = (np.array([0.0]), np.array([rain_rate]))
     return Scenario(f"valley{n}", bed, man, dx, dx, z0, z0.copy(), z0.copy(),
                     bcs=((0, 0.0),) * 4, cfl=0.5, t_end=t_end, rain=rain, sources=sources)
+
+
+def gaussian_smooth(a: np.ndarray, sigma: float) -> np.ndarray:
+    """Separable Gaussian filter (kernel truncated at 4 sigma, edges reflected)."""
+    r = int(np.ceil(4.0 * sigma))
+    x = np.arange(-r, r + 1, dtype=np.float64)
+    k = np.exp(-x * x / (2.0 * sigma * sigma))
+    k /= k.sum()
+    out = a
+    for axis in (0, 1):
+        p = np.pad(out, [(r, r) if ax == axis else (0, 0) for ax in (0, 1)], mode="reflect")
+        acc = np.zeros_like(out)
+        n = out.shape[axis]
+        for i, w in enumerate(k):
+            acc += w * (p[i:i + n, :] if axis == 0 else p[:, i:i + n])
+        out = acc
+    return out
+
+
+def lognormal_manning(n: int, seed: int, median: float = 0.04, sigma: float = 0.3,
+                      corr_cells: float = 10.0) -> np.ndarray:
+    """Per-cell Manning field with log n = ln(median) + sigma * g, g a smooth
+    Gaussian field: white noise (Box-Muller on the seeded uniforms) filtered by
+    a Gaussian of `corr_cells` cells and rescaled to unit variance."""
+    u1 = uniform(seed, 7, n * n)
+    u2 = uniform(seed, 8, n * n)
+    w = (np.sqrt(-2.0 * np.log1p(-u1)) * np.cos(2.0 * np.pi * u2)).reshape(n, n)
+    g = gaussian_smooth(w, corr_cells)
+    g = (g - g.mean()) / g.std()
+    return np.exp(np.log(median) + sigma * g)
+
+
+@dataclass
+class CalibrationProblem:
+    """Gauge-misfit calibration of the Manning field on a valley flood."""
+    scenario: Scenario        # its manning is the starting field
+    n_steps: int
+    gauges: np.ndarray        # row-major cell indices
+    manning_true: np.ndarray  # hidden field that makes the observations
+
+
+def calibration_problem(n: int = 512, dx: float = 5.0, seed: int = 0, n_steps: int = 2000,
+                        n_gauges: int = 16, hidden_seed: Optional[int] = None,
+                        t_end: float = 1.0e9) -> CalibrationProblem:
+    """The valley flood (bed, inflow, rain, open sides as `valley`) with a
+    log-normal Manning field (median 0.04, sigma 0.3, smoothed over 10 cells)
+    to calibrate against gauge depths made with a hidden field of the same
+    law. Gauges: `n_gauges` seeded rows of the valley's middle three
+    quarters, each at the lowest bed cell within n/16 of the thalweg column
+    (n/2), which the inflow and rain wet first. The run is `n_steps` steps
+    (t_end far away)."""
+    s = valley(n, dx, seed, t_end=t_end)
+    s.manning = lognormal_manning(n, seed)
+    hidden = lognormal_manning(n, seed + 1000 if hidden_seed is None else hidden_seed)
+    rows = np.unique((uniform(seed, 9, 4 * n_gauges) * (0.75 * n)).astype(int) + n // 8)
+    rows = np.sort(rows[:n_gauges])
+    w = max(n // 16, 1)
+    c0 = n // 2
+    cols = [c0 - w + int(np.argmin(s.bed[r, c0 - w:c0 + w + 1])) for r in rows]
+    gauges = np.array([r * n + c for r, c in zip(rows, cols)], dtype=np.int64)
+    return CalibrationProblem(s, int(n_steps), gauges, hidden)
 
 
 def simulation_for(s: Scenario, device: int = 0, integrator=None):

@@ -249,6 +249,58 @@ int hf_server_collect(hf_server* server, int slot, double* h, double* hu, double
 int hf_server_usage(const hf_server* server, uint64_t* bytes_in_use, int* occupied);
 
 /* ---------------------------------------------------------------------------
+ * Differentiation with respect to the per-cell Manning field.
+ *
+ * The reference differentiates by running its generic step with T = Dual
+ * (autograd/src/dual.rs; e.g. examples/m1_inverse_manning_demo.rs): forward
+ * mode, one direction per run, dt taken from values (update.rs:113-136).
+ * hf_tangent is that forward mode on the GPU with the same Dual rules
+ * (branches on values, max/min ties average the derivatives, sqrt(0) has
+ * derivative 0, powf's n x^(n-1)). hf_grad_manning is reverse mode, which the
+ * reference does not have: the gradient with respect to every Manning value
+ * (and the initial state) from one forward and one backward sweep, with
+ * checkpoints every `checkpoint_every` steps and the steps in between
+ * recomputed. It is the transpose of the tangent map: for any direction v,
+ * dot(gradient, v) equals hf_tangent's dJ along v up to rounding.
+ *
+ * A problem is a scenario (mesh, initial state, config, forcings, horizon
+ * t_end) and gauge cells (row-major indices). A run takes steps like
+ * hf_sim_run_until (dt = min(cfl dt, max_dt, t_end - t)) until t_end or
+ * n_steps steps, and its misfit is
+ *   J = sum over steps k = 1..K and gauges g of (h_k[cell_g] - h_obs[k-1][g])^2
+ * with h_obs an [n_steps][n_gauges] table (zeros until set).
+ * ------------------------------------------------------------------------- */
+typedef struct hf_calib hf_calib;
+
+int hf_calib_create(const hf_scenario_desc* scenario, int64_t n_steps, int64_t n_gauges,
+                    const int64_t* gauge_cells, int64_t checkpoint_every, int device,
+                    hf_calib** out);
+int hf_calib_destroy(hf_calib* calib);
+int hf_calib_set_observations(hf_calib* calib, const double* h_obs);
+/* Forward run with the Manning field `manning` (one value per cell). J and
+ * the gauge depths of each step ([K][n_gauges], K = *n_run) are optional
+ * outputs. With replay_dt = 0 the steps take their CFL dt and the sequence is
+ * recorded; with replay_dt != 0 they take the dt sequence recorded by the
+ * last such run (frozen dt, as the tangent and the gradient see it). */
+int hf_calib_run(hf_calib* calib, const double* manning, int replay_dt, double* J,
+                 double* gauge_h, int64_t* n_run);
+/* Forward-mode (Dual) run along the direction (dn, dh0, dhu0, dhv0); any may
+ * be NULL (zero). Returns J and its directional derivative dJ. */
+int hf_tangent(hf_calib* calib, const double* manning, const double* dn, const double* dh0,
+               const double* dhu0, const double* dhv0, double* J, double* dJ);
+/* Reverse mode: J and dJ/dn (one value per cell); the gradient with respect
+ * to the initial state is written when grad_h0 / grad_hu0 / grad_hv0 are
+ * non-NULL. */
+int hf_grad_manning(hf_calib* calib, const double* manning, double* J, double* grad_n,
+                    double* grad_h0, double* grad_hu0, double* grad_hv0);
+/* Final state of the last run, and the final tangent of the last hf_tangent
+ * (any pointer may be NULL). */
+int hf_calib_final_state(hf_calib* calib, double* h, double* hu, double* hv, double* dh,
+                         double* dhu, double* dhv);
+/* dt sequence recorded by the last run without replay (*n values). */
+int hf_calib_dt(hf_calib* calib, double* dts, int64_t* n);
+
+/* ---------------------------------------------------------------------------
  * Low-level entry points on caller-owned device buffers, mirroring the
  * reference's free functions. All run on `stream` and are asynchronous
  * unless they return a host value (hf_cfl_time_step synchronizes it).

@@ -118,3 +118,66 @@ def golden_profile(case, h):
     if case["golden_row"] is None:
         return np.round(h.reshape(-1), case["decimals"])
     return np.round(h[case["golden_row"]], case["decimals"])
+
+
+# ---------------------------------------------------------------------------
+# Forward-mode calibration demo of the reference
+# (solver-2d/examples/m1_inverse_manning_demo.rs:43-112): a 3 x 60 flat
+# channel, dx = dy = 1, h = 1 m for j < 30 and 0.1 m beyond, at rest; walls
+# north/south, transmissive west/east; uniform Manning n; SSP-RK2 with
+# dt = cfl_time_step(0.4) capped at t_end - t and Manning friction (dry_tol
+# 1e-6) after each step, to t = 20 s (at most 5000 steps). The observable is
+# the depth-weighted centroid of the middle row, sum x h / sum h with
+# x = (j + 0.5) dx, summed in column order.
+M1_ROWS, M1_COLS, M1_T_END, M1_N_TRUE, M1_N_INIT, M1_ITERS = 3, 60, 20.0, 0.040, 0.080, 12
+
+
+def m1_state():
+    h = np.where(np.arange(M1_COLS)[None, :] < M1_COLS // 2, 1.0, 0.1) * np.ones((M1_ROWS, 1))
+    z = np.zeros((M1_ROWS, M1_COLS))
+    return z, h, np.zeros_like(h), np.zeros_like(h)
+
+
+def m1_centroid(h_row, dh_row):
+    """(value, derivative) of sum x h / sum h with the Dual division rule."""
+    num = den = dnum = dden = 0.0
+    for j in range(M1_COLS):
+        x = (j + 0.5) * 1.0
+        num += h_row[j] * x
+        dnum += dh_row[j] * x
+        den += h_row[j]
+        dden += dh_row[j]
+    return num / den, (dnum * den - num * dden) / (den * den)
+
+
+def m1_newton(centroid_and_derivative):
+    """The demo's Newton iteration (m1_inverse_manning_demo.rs:124-146) given
+    n -> (centroid, d centroid / dn); returns rows (iter, n, centroid, loss,
+    dc_dn, step) and the target centroid."""
+    c_target = centroid_and_derivative(M1_N_TRUE)[0]
+    n = M1_N_INIT
+    rows = []
+    for it in range(M1_ITERS):
+        c, dc = centroid_and_derivative(n)
+        err = c - c_target
+        step = -err / dc if abs(dc) > 1e-12 else 0.0
+        rows.append((it, n, c, err * err, dc, step))
+        n = min(max(n + step, 1e-4), 1.0)
+    return np.array(rows), c_target
+
+
+def assert_matches_m1_record(rows, table, dc=0.0):
+    """Rows against the reference's CSV (n and centroid to 10 decimals, the
+    rest to 10 significant digits). `dc` is the absolute centroid difference
+    allowed between the two runs (0 when both use the same pow; a correctly
+    rounded pow moves the centroid by ~1e-14): near convergence the loss
+    err^2 and the step -err / dc_dn inherit it through err = c - c_target."""
+    assert rows.shape == table.shape
+    for got, ref in zip(rows, table):
+        it = int(ref[0])
+        assert abs(got[1] - ref[1]) <= 6e-11, (it, "n", got[1], ref[1])
+        assert abs(got[2] - ref[2]) <= 6e-11, (it, "centroid", got[2], ref[2])
+        err_tol = {3: 2.0 * np.sqrt(ref[3]) * dc + dc * dc, 4: 0.0, 5: dc / abs(ref[4])}
+        for k, name in ((3, "loss"), (4, "dc_dn"), (5, "step")):
+            tol = 6e-10 * abs(ref[k]) + err_tol[k] + 1e-22
+            assert abs(got[k] - ref[k]) <= tol, (it, name, got[k], ref[k])

@@ -1,0 +1,210 @@
+"""Differentiation on the GPU (hf_tangent, hf_grad_manning).
+
+* The DualD tangent reproduces the reference's published forward-mode
+  calibration record (m1_inverse_manning_demo.rs; 12 Newton iterations).
+* The tangent equals the oracle's Dual tangent over the same dt sequence:
+  the misfit J bit for bit (cr pow mode), dJ and the final tangent state to
+  1e-10.
+* The adjoint is the transpose of the tangent: for random directions in the
+  Manning field and the initial state, dot(gradient, direction) equals the
+  tangent's dJ; checkpoint intervals do not change the gradient (bit for
+  bit) and repeated calls are bit-identical.
+* Against central finite differences with the dt sequence frozen.
+Problems cover open, wall, discharge (with the Manning normal-depth inflow
+ghost on a dry bed) and depth boundaries, rain, point sources, wet/dry
+fronts and both integrators.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from tests import cases
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                      "reference_m1_inverse_manning.npz")
+
+
+@pytest.fixture(scope="module")
+def gpu():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from hydroflux_b200 import calib, workloads
+    return calib, workloads
+
+
+@pytest.fixture(autouse=True)
+def cr_pow(oracle):
+    oracle.set_pow_mode("cr")
+    yield
+    oracle.set_pow_mode("libm")
+
+
+def m1_scenario(workloads, n_value):
+    z, h, hu, hv = cases.m1_state()
+    return workloads.Scenario("m1", z, np.full_like(z, n_value), 1.0, 1.0, h, hu, hv,
+                              bcs=((1, 0.0), (1, 0.0), (0, 0.0), (0, 0.0)), cfl=0.4,
+                              t_end=cases.M1_T_END, max_dt=1e9)
+
+
+def test_tangent_matches_reference_newton_record(gpu):
+    calib, workloads = gpu
+    ones = np.ones((cases.M1_ROWS, cases.M1_COLS))
+    with calib.Calibration(m1_scenario(workloads, cases.M1_N_TRUE), 5000) as cal:
+        def centroid(n_value):
+            cal.tangent(n_value * ones, dn=ones)
+            st = cal.final_state()
+            return cases.m1_centroid(st["h"][1], st["dh"][1])
+        rows, _ = cases.m1_newton(centroid)
+    # The kernels' pow is correctly rounded, the reference's is the platform's.
+    cases.assert_matches_m1_record(rows, np.load(GOLDEN)["table"], dc=5e-12)
+
+
+def lognormal(rng, shape, median=0.04, sigma=0.3):
+    return median * np.exp(sigma * rng.standard_normal(shape))
+
+
+def problem(workloads, name):
+    """(scenario, n_steps, gauges)."""
+    S = workloads.Scenario
+    rng = np.random.default_rng(sum(map(ord, name)))
+    if name == "valley":  # dry start, inflow + rain, open sides
+        s = workloads.valley(n=48, dx=5.0, seed=3, peak=40.0, t_end=1e9)
+        s.manning = lognormal(rng, s.shape)
+        s.max_dt = 5.0
+        return s, 120, np.array([5 * 48 + 24, 20 * 48 + 23, 30 * 48 + 25, 40 * 48 + 24])
+    if name == "dambreak_fe":  # wet/dry dam break between walls, forward Euler, rain
+        nr, nc = 24, 40
+        x = np.arange(nc)[None, :] + 0.0 * np.arange(nr)[:, None]
+        h = np.where(x < 12, 1.5, 0.0)
+        z = 0.02 * x + 0.05 * np.sin(np.arange(nr))[:, None]
+        s = S("dambreak_fe", z, lognormal(rng, (nr, nc)), 1.0, 1.0, h, np.zeros_like(h),
+              np.zeros_like(h), bcs=((1, 0.0),) * 4, cfl=0.4, t_end=1e9, max_dt=1.0,
+              rain=(np.array([0.0]), np.array([2e-4])), integrator=0)
+        return s, 60, np.array([5 * nc + 14, 12 * nc + 20, 20 * nc + 8])
+    if name == "inflow":  # discharge onto a dry slope (normal-depth ghost), depth outlet
+        nr, nc = 20, 36
+        x = np.arange(nc)[None, :] * np.ones((nr, 1))
+        z = 2.0 - 0.02 * x + 0.1 * np.cos(0.7 * np.arange(nr))[:, None]
+        h = np.zeros((nr, nc))
+        s = S("inflow", z, lognormal(rng, (nr, nc)), 2.0, 2.0, h, h.copy(), h.copy(),
+              bcs=((1, 0.0), (1, 0.0), (2, 0.6), (3, 0.05)), cfl=0.45, t_end=1e9, max_dt=0.5,
+              sources=[(10, 20, np.array([0.0, 10.0, 40.0]), np.array([0.0, 2.0, 0.5]))])
+        return s, 150, np.array([10 * nc + 3, 5 * nc + 12, 14 * nc + 30])
+    raise KeyError(name)
+
+
+PROBLEMS = ["valley", "dambreak_fe", "inflow"]
+
+
+def observations(cal, s, n_steps, G, seed):
+    rng = np.random.default_rng(seed)
+    _, gh, k = cal.run(s.manning * np.exp(0.2 * rng.standard_normal(s.shape)))
+    obs = np.zeros((n_steps, G))
+    obs[:k] = gh
+    cal.set_observations(obs)
+    return obs
+
+
+def directions(rng, s):
+    wet = s.h > 0
+    return dict(dn=rng.standard_normal(s.shape) * 0.01,
+                dh0=rng.standard_normal(s.shape) * 0.01 * wet,
+                dhu0=rng.standard_normal(s.shape) * 0.01 * wet,
+                dhv0=rng.standard_normal(s.shape) * 0.01 * wet)
+
+
+@pytest.mark.parametrize("name", PROBLEMS)
+def test_tangent_matches_oracle(gpu, oracle, name):
+    calib, workloads = gpu
+    s, K, gauges = problem(workloads, name)
+    with calib.Calibration(s, K, gauges) as cal:
+        obs = observations(cal, s, K, len(gauges), 1)
+        d = directions(np.random.default_rng(2), s)
+        J, dJ = cal.tangent(s.manning, **d)
+        st = cal.final_state()
+        dts = cal.dts()
+    assert len(dts) == K
+    ref = oracle.tangent_run(s.bed, s.manning, d["dn"], s.dx, s.dy, s.h, s.hu, s.hv,
+                             workloads_config(s), dts, workloads.oracle_forcing(s),
+                             dh=d["dh0"], dhu=d["dhu0"], dhv=d["dhv0"], gauges=gauges,
+                             h_obs=obs.reshape(-1))
+    assert J == ref["J"]
+    assert np.array_equal(st["h"], ref["h"]) and np.array_equal(st["hu"], ref["hu"])
+    assert abs(dJ - ref["dJ"]) <= 1e-10 * abs(ref["dJ"]) + 1e-300, (dJ, ref["dJ"])
+    for k in ("dh", "dhu", "dhv"):
+        scale = np.max(np.abs(ref[k]))
+        assert np.max(np.abs(st[k] - ref[k])) <= 1e-10 * scale, k
+
+
+def workloads_config(s):
+    from hydroflux_b200.ensemble import scenario_config
+    return scenario_config(s)
+
+
+@pytest.mark.parametrize("name", PROBLEMS)
+def test_adjoint_is_transpose_of_tangent(gpu, name):
+    calib, workloads = gpu
+    s, K, gauges = problem(workloads, name)
+    with calib.Calibration(s, K, gauges, checkpoint_every=7) as cal:
+        observations(cal, s, K, len(gauges), 3)
+        J0, _, _ = cal.run(s.manning)
+        J, g, (gh, ghu, ghv) = cal.gradient(s.manning, initial_state=True)
+        assert J == J0
+        assert np.all(np.isfinite(g)) and np.any(g != 0.0)
+        rng = np.random.default_rng(4)
+        for _ in range(4):
+            d = directions(rng, s)
+            _, dJ = cal.tangent(s.manning, **d)
+            dot = (np.sum(g * d["dn"]) + np.sum(gh * d["dh0"]) + np.sum(ghu * d["dhu0"]) +
+                   np.sum(ghv * d["dhv0"]))
+            scale = (np.sum(np.abs(g * d["dn"])) + np.sum(np.abs(gh * d["dh0"])) +
+                     np.sum(np.abs(ghu * d["dhu0"])) + np.sum(np.abs(ghv * d["dhv0"])))
+            assert abs(dot - dJ) <= 1e-9 * max(abs(dJ), scale), (dot, dJ, scale)
+
+
+def test_gradient_independent_of_checkpoints_and_deterministic(gpu):
+    calib, workloads = gpu
+    s, K, gauges = problem(workloads, "valley")
+    grads = []
+    for every in (1, 7, 45, 1000):
+        with calib.Calibration(s, K, gauges, checkpoint_every=every) as cal:
+            observations(cal, s, K, len(gauges), 5)
+            grads.append(cal.gradient(s.manning)[1])
+            if every == 7:
+                assert np.array_equal(grads[-1], cal.gradient(s.manning)[1])
+    for g in grads[1:]:
+        assert np.array_equal(g, grads[0])
+
+
+def test_gradient_against_central_differences(gpu):
+    """Smooth, all-wet case; dt frozen to the base run (the gradient's dt)."""
+    calib, workloads = gpu
+    nr, nc = 32, 32
+    xx, yy = np.meshgrid(np.arange(nc) + 0.5, np.arange(nr) + 0.5)
+    h = 1.0 + 0.4 * np.exp(-((xx - 14) ** 2 + (yy - 17) ** 2) / 30.0)
+    z = 0.01 * xx
+    rng = np.random.default_rng(6)
+    n = lognormal(rng, (nr, nc), median=0.05)
+    s = workloads.Scenario("bump", z, n, 1.0, 1.0, h, np.zeros_like(h), np.zeros_like(h),
+                           bcs=((0, 0.0),) * 4, cfl=0.4, t_end=1e9, max_dt=1.0)
+    K, gauges = 40, np.array([5 * nc + 5, 16 * nc + 16, 25 * nc + 9])
+    with calib.Calibration(s, K, gauges) as cal:
+        obs = np.zeros((K, len(gauges)))
+        obs[:] = 1.1
+        cal.set_observations(obs)
+        J, g = cal.gradient(n)
+        for k in range(3):
+            v = rng.standard_normal(n.shape)
+            ad = float(np.sum(g * n * v))  # relative perturbation n (1 + eps v)
+            # eps = 1e-6: J's rounding (~1e-15 |J|) over eps is ~1e-6 of dJ, and
+            # the limiter's branch switches make J piecewise smooth, so a larger
+            # eps does not help (1e-4 is off by ~3e-5); 2e-5 bounds both.
+            eps = 1e-6
+            Jp, _, _ = cal.run(n + eps * n * v, replay_dt=True)
+            Jm, _, _ = cal.run(n - eps * n * v, replay_dt=True)
+            fd = (Jp - Jm) / (2 * eps)
+            assert abs(fd - ad) <= 2e-5 * abs(ad), (k, fd, ad)
