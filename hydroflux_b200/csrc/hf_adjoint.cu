@@ -109,6 +109,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_stage_adj(const StageArgs A, co
   const double dt_dx = dt / dx;
   const double dt_dy = dt / dy;
   const double half_dx = 0.5 * dx, half_dy = 0.5 * dy;
+  const double inv_dx = 1.0 / dx, inv_dy = 1.0 / dy;
   const int tid = threadIdx.x;
   const int ntiles = A.tiles_x * A.tiles_y;
 
@@ -270,7 +271,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_stage_adj(const StageArgs A, co
         // bed source s = (hfl + hfr) ((eta_l - hfl) - (eta_r - hfr)) (g/2) / dx
         double L_eta = 0.0, L_sex = 0.0, L_sey = 0.0;
         {
-          const double kx = hfa::div_rn(L_shu * (0.5 * GRAVITY), dx);
+          const double kx = L_shu * (0.5 * GRAVITY) * inv_dx;
           const double Aa = hfl + hfr, Bb = (eta_left - hfl) - (eta_right - hfr);
           const double LA = kx * Bb, LB = kx * Aa;
           const double L_hfl = LA - LB, L_hfr = LA + LB;
@@ -281,7 +282,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_stage_adj(const StageArgs A, co
           if (gj + 1 < nc) L_sex += L_er * (0.5 * dx);
         }
         {
-          const double ky = hfa::div_rn(L_shv * (0.5 * GRAVITY), dy);
+          const double ky = L_shv * (0.5 * GRAVITY) * inv_dy;
           const double Aa = hft + hfb, Bb = (eta_top - hft) - (eta_bot - hfb);
           const double LA = ky * Bb, LB = ky * Aa;
           const double L_hft = LA - LB, L_hfb = LA + LB;
@@ -338,9 +339,9 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_stage_adj(const StageArgs A, co
       const double xa = S.h[i4(li, lj)] - H_DRY;
       const double avail = fmax(xa, 0.0);
       if (out > avail && out > 0.0) {  // alpha = avail / out
-        const double alpha = hfa::div_rn(avail, out);
-        R.ldir[0][k] += hfa::div_rn(L_a, out) * dmax0(xa);
-        R.lout[k] = -hfa::div_rn(L_a * alpha, out);
+        const double inv_out = 1.0 / out;
+        R.ldir[0][k] += L_a * inv_out * dmax0(xa);
+        R.lout[k] = -L_a * avail * inv_out * inv_out;
       }
     }
     __syncthreads();
@@ -559,6 +560,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_stage_adj(const StageArgs A, co
           const int na = xd ? nc : nr;
           if (na < 2) continue;
           const double d = xd ? dx : dy;
+          const double inv_d = xd ? inv_dx : inv_dy;
           for (int o = -1; o <= 1; ++o) {
             const int si = xd ? li : li + o, sj = xd ? lj + o : lj;  // slope cell
             const bool in_reg = xd ? (si >= -1 && si <= TY && sj >= -2 && sj <= TX + 1)
@@ -598,9 +600,9 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_stage_adj(const StageArgs A, co
               }
               ce = cc[0]; cu = cc[1]; cv = cc[2];
             }
-            le += hfa::div_rn(ce * Le, d);
-            lu += hfa::div_rn(cu * Lu, d);
-            lv += hfa::div_rn(cv * Lv, d);
+            le += ce * Le * inv_d;
+            lu += cu * Lu * inv_d;
+            lv += cv * Lv * inv_d;
           }
         }
         // primitives: eta = h + z, u = hu / h, v = hv / h (when h > H_VEL)
@@ -608,9 +610,10 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_stage_adj(const StageArgs A, co
         oh = le;
         if (hh > H_VEL) {
           const double uu = S.u[k], vv = S.v[k];
-          ohu = hfa::div_rn(lu, hh);
-          ohv = hfa::div_rn(lv, hh);
-          oh -= hfa::div_rn(lu * uu + lv * vv, hh);
+          const double inv = 1.0 / hh;
+          ohu = lu * inv;
+          ohv = lv * inv;
+          oh -= (lu * uu + lv * vv) * inv;
         }
         if (in_alpha(li, lj)) {
           const int ca = ia(li, lj);

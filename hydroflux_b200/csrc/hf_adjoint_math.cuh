@@ -5,7 +5,10 @@
 // forward intermediates and branches exactly as the forward code does, and
 // maps the adjoint of the outputs to the adjoint of the arguments: the
 // transpose of the derivative that the reference's Dual arithmetic
-// (autograd/src/dual.rs) propagates through the same code. Ties of max/min
+// (autograd/src/dual.rs) propagates through the same code. Values that
+// decide a branch are recomputed with the forward's exact operations; values
+// that only scale adjoints use one shared reciprocal per denominator (the
+// adjoint is a derivative, not a bit-exact quantity). Ties of max/min
 // split the adjoint in halves (dual.rs:130-155), sqrt at 0 passes none
 // (dual.rs:46-50), powf contributes n x^(n-1) (dual.rs:112-117).
 #pragma once
@@ -69,7 +72,10 @@ HF_ADJ_HD void hllc_normal_rev(double h_l, double qn_l, double qt_l, double h_r,
   const double qt = left ? qt_l : qt_r;
   const double un = left ? un_l : un_r;
   const bool wet = left ? wl : wr;
-  const double ut = wet ? hfa::div_rn(qt, h) : 0.0;
+  const double inv_hl = wl ? 1.0 / h_l : 0.0;
+  const double inv_hr = wr ? 1.0 / h_r : 0.0;
+  const double inv_h = left ? inv_hl : inv_hr;
+  const double ut = wet ? qt * inv_h : 0.0;
 
   double L_h = 0.0, L_qn = 0.0, L_qt = 0.0, L_un = 0.0, L_ut = 0.0;  // picked side
   double L_sl = 0.0, L_sr = 0.0, L_ss = 0.0;
@@ -77,7 +83,8 @@ HF_ADJ_HD void hllc_normal_rev(double h_l, double qn_l, double qt_l, double h_r,
     // o = f + (hs - h) s, (hs s* - qn) s, (hs ut - qt) s; hs = h (s - un) / (s - s*)
     const double s = left ? sl : sr;
     const double D = s - s_star;
-    const double hs = hfa::div_rn(h * (s - un), D);
+    const double inv_D = 1.0 / D;
+    const double hs = h * (s - un) * inv_D;
     const double L_hs = Lm * s + Ln * s_star * s + Lt * ut * s;
     double L_s = Lm * (hs - h) + Ln * (hs * s_star - qn) + Lt * (hs * ut - qt);
     L_h -= Lm * s;
@@ -85,8 +92,8 @@ HF_ADJ_HD void hllc_normal_rev(double h_l, double qn_l, double qt_l, double h_r,
     L_qn -= Ln * s;
     L_ut += Lt * hs * s;
     L_qt -= Lt * s;
-    const double L_N = hfa::div_rn(L_hs, D);
-    const double L_D = -hfa::div_rn(L_hs * hs, D);
+    const double L_N = L_hs * inv_D;
+    const double L_D = -L_hs * hs * inv_D;
     L_h += L_N * (s - un);
     L_s += L_N * h;
     L_un -= L_N * h;
@@ -100,8 +107,8 @@ HF_ADJ_HD void hllc_normal_rev(double h_l, double qn_l, double qt_l, double h_r,
     L_un += Ln * qn;
     L_h += Ln * (2.0 * h) * (0.5 * GRAVITY);
     L_ut += Lt * qn;
-    L_qt += hfa::div_rn(L_ut, h);
-    L_h -= hfa::div_rn(L_ut * ut, h);
+    L_qt += L_ut * inv_h;
+    L_h -= L_ut * ut * inv_h;
   }
   double L_unl = 0.0, L_unr = 0.0;
   if (left) {
@@ -113,8 +120,9 @@ HF_ADJ_HD void hllc_normal_rev(double h_l, double qn_l, double qt_l, double h_r,
     if (fabs(denom) > 1.0e-12) {
       // s* = (a1 sl - b1 sr) / (a1 - b1), a1 = h_r (un_r - sr), b1 = h_l (un_l - sl)
       const double a1 = h_r * (un_r - sr), b1 = h_l * (un_l - sl);
-      const double L_num = hfa::div_rn(L_ss, denom);
-      const double L_den = -hfa::div_rn(L_ss * s_star, denom);
+      const double inv_den = 1.0 / denom;
+      const double L_num = L_ss * inv_den;
+      const double L_den = -L_ss * s_star * inv_den;
       const double L_a1 = L_num * sl + L_den;
       const double L_b1 = -L_num * sr - L_den;
       L_sl += L_num * a1;
@@ -151,15 +159,13 @@ HF_ADJ_HD void hllc_normal_rev(double h_l, double qn_l, double qt_l, double h_r,
     L_unl += L_sl + L_sr;
     L_cl += 2.0 * L_sr - L_sl;
   }
-  if (wl) {  // un_l = qn_l / h_l, cl = sqrt(g h_l)
-    L_qnl += hfa::div_rn(L_unl, h_l);
-    L_hl -= hfa::div_rn(L_unl * un_l, h_l);
-    L_hl += hfa::div_rn(L_cl * GRAVITY, 2.0 * cl);
+  if (wl) {  // un_l = qn_l / h_l; cl = sqrt(g h_l), dcl/dh = g / (2 cl) = cl / (2 h_l)
+    L_qnl += L_unl * inv_hl;
+    L_hl += (L_cl * (0.5 * cl) - L_unl * un_l) * inv_hl;
   }
   if (wr) {
-    L_qnr += hfa::div_rn(L_unr, h_r);
-    L_hr -= hfa::div_rn(L_unr * un_r, h_r);
-    L_hr += hfa::div_rn(L_cr * GRAVITY, 2.0 * cr);
+    L_qnr += L_unr * inv_hr;
+    L_hr += (L_cr * (0.5 * cr) - L_unr * un_r) * inv_hr;
   }
 }
 
@@ -195,16 +201,16 @@ HF_ADJ_HD void wb_face_rev(double hL, double qnL, double qtL, double hR,
   LhL += L_hsL * dmax0(xL);
   LhR += L_hsR * dmax0(xR);
   if (hL > H_VEL) {  // qns = hs * (qn / h)
-    const double LunL = a1 * hsL, LutL = a2 * hsL;
-    LqnL += hfa::div_rn(LunL, hL);
-    LqtL += hfa::div_rn(LutL, hL);
-    LhL -= hfa::div_rn(LunL * unL + LutL * utL, hL);
+    const double LunL = a1 * hsL, LutL = a2 * hsL, inv = 1.0 / hL;
+    LqnL += LunL * inv;
+    LqtL += LutL * inv;
+    LhL -= (LunL * unL + LutL * utL) * inv;
   }
   if (hR > H_VEL) {
-    const double LunR = b1 * hsR, LutR = b2 * hsR;
-    LqnR += hfa::div_rn(LunR, hR);
-    LqtR += hfa::div_rn(LutR, hR);
-    LhR -= hfa::div_rn(LunR * unR + LutR * utR, hR);
+    const double LunR = b1 * hsR, LutR = b2 * hsR, inv = 1.0 / hR;
+    LqnR += LunR * inv;
+    LqtR += LutR * inv;
+    LhR -= (LunR * unR + LutR * utR) * inv;
   }
 }
 
@@ -250,32 +256,36 @@ HF_ADJ_HD void ghost_rev(int side, const BcDev& bc, double h,
 // adjoint (Lhu, Lhv) of the post-friction momentum is replaced by that of the
 // pre-friction state; Lh and Ln are added to.
 HF_ADJ_HD void friction_rev(double h, double hu, double hv, double n, double dt,
-                                             double dry_tol, double& Lh, double& Lhu, double& Lhv,
-                                             double& Ln) {
+                             double dry_tol, double& Lh, double& Lhu, double& Lhv, double& Ln) {
   if (h <= dry_tol) return;
   if (n == 0.0) return;
+  // Forward values (they only scale adjoints): speed = |q| / h,
+  // A = n^2 speed / h^(4/3), factor = A dt g + 1, hu' = hu / factor.
   const double dt_g = dt * GRAVITY;
+  const double inv_h = 1.0 / h;
   const double S = hfa::sqrt_rn(hu * hu + hv * hv);
-  const double speed = hfa::div_rn(S, h);
-  const double P = hfpow::pow_4_3(h);
-  const double A = hfa::div_rn(n * n * speed, P);
-  const double factor = A * dt_g + 1.0;
-  const double hu1 = hfa::div_rn(hu, factor), hv1 = hfa::div_rn(hv, factor);
-  const double L_factor = -hfa::div_rn(Lhu * hu1 + Lhv * hv1, factor);
-  const double nLhu = hfa::div_rn(Lhu, factor), nLhv = hfa::div_rn(Lhv, factor);
+  const double speed = S * inv_h;
+  // d h^e / dh = e h^(e-1) (dual.rs:112-117) with e = fl(4/3); cbrt(h) is
+  // h^(e-1) to within 1e-15 relative (e - 1 = 1/3 - 7.4e-17).
+  const double e = 4.0 / 3.0;
+  const double q = cbrt(h);
+  const double inv_P = 1.0 / (h * q);
+  const double A = n * n * speed * inv_P;
+  const double inv_f = 1.0 / (A * dt_g + 1.0);
+  const double L_factor = -(Lhu * hu + Lhv * hv) * inv_f * inv_f;
+  const double nLhu = Lhu * inv_f, nLhv = Lhv * inv_f;
   const double L_A = L_factor * dt_g;
-  const double L_N2S = hfa::div_rn(L_A, P);  // n n speed
-  const double L_P = -hfa::div_rn(L_A * A, P);
+  const double L_N2S = L_A * inv_P;  // adjoint of n n speed
+  const double L_P = -L_A * A * inv_P;
   Ln += L_N2S * (2.0 * n) * speed;
   const double L_speed = L_N2S * n * n;
-  const double e = 4.0 / 3.0;
-  Lh += L_P * (e * pow(h, e - 1.0));
-  const double L_S = hfa::div_rn(L_speed, h);
-  Lh -= hfa::div_rn(L_speed * speed, h);
+  Lh += L_P * (e * q);
+  const double L_S = L_speed * inv_h;
+  Lh -= L_speed * speed * inv_h;
   Lhu = nLhu;
   Lhv = nLhv;
   if (S != 0.0) {  // sqrt(0) passes no derivative (dual.rs:46-50)
-    const double L_Q = hfa::div_rn(L_S, 2.0 * S);
+    const double L_Q = L_S * (0.5 / S);
     Lhu += L_Q * (2.0 * hu);
     Lhv += L_Q * (2.0 * hv);
   }

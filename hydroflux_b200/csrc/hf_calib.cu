@@ -87,6 +87,7 @@ struct hf_calib {
   int64_t nr = 0, nc = 0, ncell = 0;
   int tiles_x = 0, tiles_y = 0, ntiles = 0;
   int grid = 1, grid_dual = 1, grid_adj = 1;
+  int grid_tiles = 1;  // one CTA per tile: the two backward streams share the SMs
   double dx = 1.0, dy = 1.0, t_end = 0.0;
   hf_config cfg;
   int64_t K = 0, G = 0, C = 1;
@@ -351,12 +352,13 @@ int recompute_segment(hf_calib* c, int64_t j, int b) {
       s1[f] = slot(buf, c->C + 1 + i, f, nb);
     }
     C_TRY(launch_control(c->ctrl_rec, c->dx, c->dy, fd, st));
-    C_TRY(launch_stage(calib_args(c, su, s1, nullptr, 0, 0, c->ctrl_rec, fd), c->grid, st));
+    C_TRY(launch_stage(calib_args(c, su, s1, nullptr, 0, 0, c->ctrl_rec, fd), c->grid_tiles, st));
     if (ssp)  // stage 2 writes U^{k+1} to the next slot (combining with U^k of this slot)
-      C_TRY(launch_stage(calib_args(c, s1, su_next, su, 1, 1, c->ctrl_rec, fd), c->grid, st));
+      C_TRY(launch_stage(calib_args(c, s1, su_next, su, 1, 1, c->ctrl_rec, fd), c->grid_tiles,
+                         st));
     else
-      C_TRY(launch_finalize(calib_args(c, s1, su_next, nullptr, 0, 1, c->ctrl_rec, fd), c->grid,
-                            st));
+      C_TRY(launch_finalize(calib_args(c, s1, su_next, nullptr, 0, 1, c->ctrl_rec, fd),
+                            c->grid_tiles, st));
   }
   C_CUDA(cudaEventRecord(c->ev_rec[b], st));
   return HF_OK;
@@ -384,18 +386,18 @@ int reverse_segment(hf_calib* c, int64_t j, int b) {
     if (ssp) {
       C_TRY(launch_stage_adj(calib_args(c, s1, nullptr, su, 1, 1, c->ctrl_rev, fd), c->lam[0],
                              c->lam[1], c->lam[2], c->lamun[0], c->lamun[1], c->lamun[2],
-                             c->halo, c->grid_adj, st));
+                             c->halo, c->grid_tiles, st));
       C_TRY(launch_adj_gather(nr, nc, c->tiles_x, c->tiles_y, c->halo, nullptr, nullptr, nullptr,
                               c->lam1[0], c->lam1[1], c->lam1[2], c->grad, st));
       C_TRY(launch_stage_adj(calib_args(c, su, nullptr, nullptr, 0, 0, c->ctrl_rev, fd),
                              c->lam1[0], c->lam1[1], c->lam1[2], nullptr, nullptr, nullptr,
-                             c->halo, c->grid_adj, st));
+                             c->halo, c->grid_tiles, st));
       C_TRY(launch_adj_gather(nr, nc, c->tiles_x, c->tiles_y, c->halo, c->lamun[0], c->lamun[1],
                               c->lamun[2], c->lam[0], c->lam[1], c->lam[2], c->grad, st));
     } else {
       C_TRY(launch_stage_adj(calib_args(c, su, nullptr, nullptr, 0, 1, c->ctrl_rev, fd),
                              c->lam[0], c->lam[1], c->lam[2], nullptr, nullptr, nullptr, c->halo,
-                             c->grid_adj, st));
+                             c->grid_tiles, st));
       C_TRY(launch_adj_gather(nr, nc, c->tiles_x, c->tiles_y, c->halo, nullptr, nullptr, nullptr,
                               c->lam[0], c->lam[1], c->lam[2], c->grad, st));
     }
@@ -567,7 +569,8 @@ int hf_calib_create(const hf_scenario_desc* d, int64_t n_steps, int64_t n_gauges
     return bail(rc);
   c->grid = stage_grid_size(c->ntiles, device);
   c->grid_dual = stage_dual_grid_size(c->ntiles, device);
-  c->grid_adj = adj_grid_size(c->ntiles, device);
+  c->grid_adj = adj_grid_size(c->ntiles, device);  // also sets the kernel's smem limit
+  c->grid_tiles = c->ntiles;
   if (cudaGetLastError() != cudaSuccess) return bail(cfail(HF_ERR_CUDA, "kernel attributes"));
   *out = c;
   return HF_OK;
