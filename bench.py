@@ -48,9 +48,22 @@ def parse():
     p.add_argument("--cpu-steps", type=int, default=2, help="oracle steps in the CPU baseline")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--workload", default="valley", choices=["valley", "ensemble"],
+    p.add_argument("--workload", default="valley", choices=["valley", "ensemble", "adjoint",
+                                                            "serve"],
                    help="valley: the 4096^2 plain step (default line); ensemble: batched "
-                        "uneven-size scenarios vs a loop of per-scenario solves")
+                        "uneven-size scenarios vs a loop of per-scenario solves; adjoint: "
+                        "misfit gradient w.r.t. the Manning field vs the forward solve; "
+                        "serve: an arrival stream through the continuous-batching server vs "
+                        "a sequential plain solve per request")
+    p.add_argument("--calib-n", type=int, default=512, help="adjoint: grid side")
+    p.add_argument("--calib-steps", type=int, default=2000, help="adjoint: steps of the misfit")
+    p.add_argument("--checkpoint-every", type=int, default=45)
+    p.add_argument("--requests", type=int, default=200, help="serve: requests in the stream")
+    p.add_argument("--rate", type=float, default=50.0, help="serve: arrivals per second")
+    p.add_argument("--sides", default="64,128,256,512", help="serve: grid sides (uniform)")
+    p.add_argument("--horizon", default="60,300", help="serve: horizon range in s (uniform)")
+    p.add_argument("--max-active-cells", type=int, default=1 << 20,
+                   help="serve: cells advancing together (admission cap)")
     p.add_argument("--scenarios", type=int, default=512)
     p.add_argument("--loop-every", type=int, default=8,
                    help="ensemble: the per-scenario loop times every k-th scenario")
@@ -60,40 +73,7 @@ def parse():
 
 
 # --------------------------------------------------------------------- dist
-class Dist:
-    def __init__(self, use_gpu: bool):
-        self.world = int(os.environ.get("WORLD_SIZE", "1"))
-        self.rank = int(os.environ.get("RANK", "0"))
-        self.local = int(os.environ.get("LOCAL_RANK", "0"))
-        self.pg = False
-        if self.world > 1 and use_gpu:
-            import datetime
-
-            import torch
-            import torch.distributed as dist
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                    device_id=torch.device("cuda", self.local))
-            self.pg = True
-
-    def barrier(self):
-        if self.pg:
-            import torch.distributed as dist
-            dist.barrier()
-
-    def max(self, x: float) -> float:
-        if not self.pg:
-            return x
-        import torch
-        import torch.distributed as dist
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    def close(self):
-        if self.pg:
-            import torch.distributed as dist
-            dist.destroy_process_group()
+from hydroflux_b200.dist import Dist  # noqa: E402  (ranks, barrier, max over ranks, sharding)
 
 
 # ------------------------------------------------------------------- clocks
@@ -367,8 +347,8 @@ def run_reference(a, d: Dist):
 def run_ensemble(a, d: Dist):
     """Batched ensemble (hf_batch_*) against a loop of per-scenario plain GPU
     solves (hf_sim run_steps, one scenario after another), same scenarios and
-    the same number of steps per scenario. Scenarios are sharded over ranks
-    (every world-th scenario per rank; no collective)."""
+    the same number of steps per scenario. Scenarios are sharded over ranks by
+    cell count (longest first to the lightest rank; no collective)."""
     import torch
 
     from hydroflux_b200 import _lib, workloads
@@ -378,7 +358,7 @@ def run_ensemble(a, d: Dist):
     _lib.lib()
     t_gen = time.perf_counter()
     allscn = ensemble_scenarios(count=a.scenarios, seed=0)
-    mine = allscn[d.rank::d.world]
+    mine = [allscn[i] for i in d.shard([s.n_cells for s in allscn])]
     gen_s = time.perf_counter() - t_gen
     cells = np.array([s.n_cells for s in mine], dtype=np.float64)
     ens = Ensemble(mine, device=dev)
@@ -395,7 +375,7 @@ def run_ensemble(a, d: Dist):
     st1 = np.array([ens.info(k)["steps"] for k in range(len(mine))], dtype=np.float64)
     el = d.max(t1 - t0)
     batched = float(np.sum(cells * (st1 - st0)))
-    batched_rate = d.world * batched / el
+    batched_rate = d.sum(batched) / el
     complete = None
     if a.complete:
         t2 = time.perf_counter()
@@ -422,7 +402,7 @@ def run_ensemble(a, d: Dist):
     loop_rate = loop_cells / loop_time if loop_time > 0 else None
     line = {"metric": "ensemble cell-updates/s (batched)", "value": batched_rate,
             "unit": "cell-updates/s", "n_gpus": d.world, "steps": a.steps,
-            "warmup": max(a.warmup, 3), "higher_is_better": True, "scaling": "weak",
+            "warmup": max(a.warmup, 3), "higher_is_better": True, "scaling": "strong",
             "dtype": "f64", "data": "synthetic (seeded valley ensemble)",
             "config": {"workload": f"{a.scenarios} scenarios, side log-uniform in [64, 1024], "
                                    "valley DEM per-scenario seed, n ~ U[0.02, 0.08], inflow "
@@ -438,6 +418,217 @@ def run_ensemble(a, d: Dist):
         print(json.dumps(line), flush=True)
 
 
+def run_adjoint(a, d: Dist):
+    """Gradient of the gauge misfit with respect to the per-cell Manning field
+    (hf_grad_manning, checkpointed adjoint) against the forward solve of the
+    same misfit (hf_calib_run) and a plain solve of the same steps (hf_sim
+    run_steps); checked against the Dual tangent in 8 seeded Gaussian
+    directions and against central differences (eps = 1e-6, dt frozen).
+    Replicas on N > 1 (each rank its own copy; max over ranks)."""
+    import torch
+
+    from hydroflux_b200 import _lib, calib, workloads
+    dev = d.local
+    torch.cuda.set_device(dev)
+    _lib.lib()
+    P = workloads.calibration_problem(n=a.calib_n, n_steps=a.calib_steps)
+    s = P.scenario
+    K = P.n_steps
+    reps = min(max(a.steps, 1), 5)  # each repetition is a full forward + gradient
+    with calib.Calibration(s, K, P.gauges, checkpoint_every=a.checkpoint_every,
+                           device=dev) as cal:
+        _, gh, k_obs = cal.run(P.manning_true)
+        obs = np.zeros((K, len(P.gauges)))
+        obs[:k_obs] = gh
+        cal.set_observations(obs)
+        for _ in range(max(a.warmup, 3) if a.warmup else 1):
+            cal.run(s.manning)
+            cal.gradient(s.manning)
+        torch.cuda.synchronize(dev)
+        d.barrier()
+        clocks = ClockSampler(dev)
+        clocks.start()
+        t_fwd, t_grad = [], []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            J, _, k_run = cal.run(s.manning)
+            t1 = time.perf_counter()
+            Jg, g = cal.gradient(s.manning)
+            t2 = time.perf_counter()
+            t_fwd.append(t1 - t0)
+            t_grad.append(t2 - t1)
+        clk = clocks.stop()
+        f_s = d.max(statistics.median(t_fwd))
+        g_s = d.max(statistics.median(t_grad))
+        # checks: Dual tangent in 8 directions, central differences in 2
+        rng = np.random.default_rng(12345)
+        dot_errs, t_tan = [], []
+        for _ in range(8):
+            v = rng.standard_normal(s.shape) * s.manning * 0.01
+            t0 = time.perf_counter()
+            _, dJ = cal.tangent(s.manning, dn=v)
+            t_tan.append(time.perf_counter() - t0)
+            ad = float(np.sum(g * v))
+            dot_errs.append(abs(ad - dJ) / max(abs(dJ), 1e-300))
+        fd_errs = []
+        cal.run(s.manning)  # dt record of the base field
+        for _ in range(2):
+            v = rng.standard_normal(s.shape) * s.manning
+            eps = 1e-6
+            Jp, _, _ = cal.run(s.manning + eps * v, replay_dt=True)
+            Jm, _, _ = cal.run(s.manning - eps * v, replay_dt=True)
+            fd = (Jp - Jm) / (2 * eps)
+            ad = float(np.sum(g * v))
+            fd_errs.append({"fd": fd, "adjoint": ad, "rel": abs(fd - ad) / max(abs(ad), 1e-300)})
+    with workloads.simulation_for(s, device=dev) as sm:
+        sm.run_steps(3, s.t_end)
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        sm.run_steps(K, s.t_end)
+        torch.cuda.synchronize(dev)
+        plain_s = d.max(time.perf_counter() - t0)
+    # Where the linearization stops predicting: adjoint vs central differences
+    # and the size of the tangent state, by misfit horizon.
+    by_horizon = []
+    for Kh in (h for h in (50, 100, 200, 500, 1000, 2000) if h <= K):
+        Ph = workloads.calibration_problem(n=a.calib_n, n_steps=Kh)
+        with calib.Calibration(Ph.scenario, Kh, Ph.gauges, checkpoint_every=a.checkpoint_every,
+                               device=dev) as ch:
+            _, gh, ko = ch.run(Ph.manning_true)
+            ob = np.zeros((Kh, len(Ph.gauges)))
+            ob[:ko] = gh
+            ch.set_observations(ob)
+            Jh, gg = ch.gradient(Ph.scenario.manning)
+            rr = np.random.default_rng(777)
+            v = rr.standard_normal(Ph.scenario.shape) * Ph.scenario.manning
+            ad = float(np.sum(gg * v))
+            ch.run(Ph.scenario.manning)
+            eps = 1e-6
+            Jp, _, _ = ch.run(Ph.scenario.manning + eps * v, replay_dt=True)
+            Jm, _, _ = ch.run(Ph.scenario.manning - eps * v, replay_dt=True)
+            fd = (Jp - Jm) / (2 * eps)
+            ch.tangent(Ph.scenario.manning, dn=v)
+            st = ch.final_state()
+            by_horizon.append({"steps": Kh, "J": Jh, "adjoint": ad, "fd": fd,
+                               "rel": abs(fd - ad) / max(abs(ad), 1e-300),
+                               "max_abs_dh": float(np.max(np.abs(st["dh"])))})
+    ncell = s.n_cells
+    line = {"metric": "misfit gradient time / forward solve time", "value": g_s / f_s,
+            "unit": "x", "n_gpus": d.world, "steps": reps, "warmup": max(a.warmup, 3),
+            "higher_is_better": False, "scaling": "replicas",
+            "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded valley, log-normal Manning field, hidden-field gauges)",
+            "config": {"workload": f"Manning-field gradient of a 16-gauge misfit over {K} steps, "
+                                   f"valley {a.calib_n}x{a.calib_n}, dx 5 m, log-normal n "
+                                   "(median 0.04, sigma 0.3, 10-cell smoothing)",
+                       "cells": ncell, "misfit_steps": int(k_run),
+                       "checkpoint_every": a.checkpoint_every, "parallelism": "replicas"},
+            "gradient_s": g_s, "forward_s": f_s, "plain_solve_s": plain_s,
+            "gradient_vs_plain_solve": g_s / plain_s,
+            "tangent_s": statistics.median(t_tan), "J": Jg,
+            "checks": {"dual_tangent_8_dirs_max_rel": max(dot_errs),
+                       "central_fd_eps1e-6": fd_errs, "fd_by_horizon": by_horizon},
+            # per misfit step: primal 5, replay 3, reverse 7 launches
+            "gpu_launches": int(k_run) * 15, "clocks": clk}
+    if d.rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_serve(a, d: Dist):
+    """An arrival stream through the continuous-batching server (hf_server_*)
+    against a sequential plain solve per request (hf_sim run_until, FIFO, one
+    at a time, same requests): p50/p99 latency (arrival -> result) and
+    solves/s. The sequential server's latencies come from the measured
+    per-request solve times queued in arrival order. The stream is split over
+    ranks by work (cells x horizon, longest first to the lightest rank); rank
+    0 gathers every request's latency."""
+    import torch
+
+    from hydroflux_b200 import _lib, serve, workloads
+    dev = d.local
+    torch.cuda.set_device(dev)
+    _lib.lib()
+    sides = tuple(int(x) for x in a.sides.split(","))
+    h0, h1 = (float(x) for x in a.horizon.split(","))
+    reqs = serve.request_stream(a.requests, rate=a.rate, seed=7, sides=sides, horizon_min=h0,
+                                horizon_max=h1, max_dt=60.0)
+    t_gen = time.perf_counter()
+    for r in reqs:  # payloads (bed, n, forcings) arrive with the request
+        r.prepare()
+    gen_s = time.perf_counter() - t_gen
+    mine = [reqs[i] for i in d.shard([r.work() for r in reqs])]
+    # warm-up: one small request through each path
+    warm = serve.request_stream(2, rate=1e6, seed=99, sides=(64,), horizon_min=5.0,
+                                horizon_max=10.0)
+    serve.serve_stream(warm, hbm_budget_bytes=150 << 30, device=dev)
+    torch.cuda.synchronize(dev)
+    d.barrier()
+    clocks = ClockSampler(dev)
+    clocks.start()
+    out = serve.serve_stream(mine, hbm_budget_bytes=150 << 30, device=dev, policy="srpt",
+                             max_active_cells=a.max_active_cells)
+    clk = clocks.stop()
+    for r in mine:
+        r.admitted = r.done = r.result = None
+    fifo = serve.serve_stream(mine, hbm_budget_bytes=150 << 30, device=dev, policy="fifo")
+    # sequential plain solves in arrival order
+    ordered = sorted(mine, key=lambda q: q.arrival)
+    service = []
+    for r in ordered:
+        s = r.prepare()
+        with workloads.simulation_for(s, device=dev) as sm:
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            sm.run_until(s.t_end)
+            torch.cuda.synchronize(dev)
+            service.append(time.perf_counter() - t0)
+    t_free, lat = 0.0, []
+    for r, sv in zip(ordered, service):
+        start = max(r.arrival, t_free)
+        t_free = start + sv
+        lat.append(t_free - r.arrival)
+    # whole-job figures: latencies of every rank's requests, the slowest rank's makespan
+    per_rank = d.gather({"served": list(out["latencies"]),
+                         "fifo": list(fifo["latencies"]), "seq": lat,
+                         "makespan": out["makespan"], "fifo_makespan": fifo["makespan"],
+                         "seq_end": t_free, "busy": float(sum(service))})
+    if d.rank != 0:
+        return
+    cat = lambda k: np.concatenate([np.asarray(x[k], dtype=np.float64) for x in per_rank])  # noqa: E731
+    n_all = len(cat("served"))
+    mk = max(x["makespan"] for x in per_rank)
+    out = {"latency_p50": float(np.percentile(cat("served"), 50)),
+           "latency_p99": float(np.percentile(cat("served"), 99)),
+           "solves_per_s": n_all / mk, "makespan": mk, "failed": out["failed"]}
+    fmk = max(x["fifo_makespan"] for x in per_rank)
+    fifo = {"latency_p50": float(np.percentile(cat("fifo"), 50)),
+            "latency_p99": float(np.percentile(cat("fifo"), 99)),
+            "solves_per_s": n_all / fmk, "makespan": fmk}
+    seq_end = max(x["seq_end"] for x in per_rank)
+    seq = {"latency_p50": float(np.percentile(cat("seq"), 50)),
+           "latency_p99": float(np.percentile(cat("seq"), 99)),
+           "solves_per_s": n_all / seq_end, "busy_s": float(sum(x["busy"] for x in per_rank))}
+    line = {"metric": "served solves/s", "value": out["solves_per_s"],
+            "unit": "solves/s", "n_gpus": d.world, "steps": n_all, "warmup": 2,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded valley per request)",
+            "config": {"workload": f"Poisson stream, {a.requests} requests at {a.rate}/s, side "
+                                   f"uniform over {list(sides)}, horizon U[{h0}, {h1}] s, valley "
+                                   "DEM / n / inflow per request seed, HBM budget 150 GB",
+                       "parallelism": f"requests sharded over {d.world} GPU(s) by work"},
+            "latency_p50_s": out["latency_p50"], "latency_p99_s": out["latency_p99"],
+            "failed": out["failed"], "makespan_s": out["makespan"],
+            "admission": f"shortest work (cells x horizon) first, at most "
+                         f"{a.max_active_cells} cells advancing together",
+            "fifo_uncapped": {k: fifo[k] for k in ("latency_p50", "latency_p99",
+                                                   "solves_per_s", "makespan")},
+            "payload_generation_s": gen_s,
+            "sequential_plain": seq,
+            "speedup_solves_per_s": out["solves_per_s"] / seq["solves_per_s"],
+            "gpu_launches": None, "clocks": clk}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     a = parse()
     d = Dist(use_gpu=a.impl == "ours")
@@ -446,6 +637,10 @@ def main():
             run_reference(a, d)
         elif a.workload == "ensemble":
             run_ensemble(a, d)
+        elif a.workload == "adjoint":
+            run_adjoint(a, d)
+        elif a.workload == "serve":
+            run_serve(a, d)
         else:
             run_ours(a, d)
     finally:

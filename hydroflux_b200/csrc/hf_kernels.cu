@@ -2,7 +2,7 @@
 //
 // The reference (franciscoparrao/hydroflux, solver-2d/src/update.rs:805-1211)
 // runs one forward-Euler stage as eleven full-grid passes over a ~241 B/cell
-// workspace. Here one stage is ONE kernel: a CTA stages a 32x16 tile plus a
+// workspace. Here one stage is ONE kernel: a CTA stages a 32x8 tile plus a
 // 4-cell halo of (h, z, eta, u, v) in shared memory and runs every pass of
 // the stage on it -- dry snapshot, primitives, limited slopes, face beds,
 // Audusse+HLLC faces, alpha rescaling, FV update with the bed source and the

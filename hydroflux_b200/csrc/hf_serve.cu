@@ -367,7 +367,10 @@ int hf_server_advance(hf_server* v, uint64_t n_batch_steps, int* n_finished) {
     S_TRY(build_serve_graph(v, which));
     S_CUDA(cudaGraphLaunch(v->graphs[which], v->stream));
     left -= (uint64_t)kServeChunk[which];
-    S_CUDA(cudaMemcpyAsync(v->h_ctrl, v->d_ctrl, v->max_slots * sizeof(Ctrl), cudaMemcpyDeviceToHost,
+    int top = 0;  // control blocks past the highest used slot are idle
+    for (int k = 0; k < v->max_slots; ++k)
+      if (v->slots[k].used) top = k + 1;
+    S_CUDA(cudaMemcpyAsync(v->h_ctrl, v->d_ctrl, top * sizeof(Ctrl), cudaMemcpyDeviceToHost,
                            v->stream));
     S_CUDA(cudaStreamSynchronize(v->stream));
     waiting = refresh_finished(v);

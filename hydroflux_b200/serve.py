@@ -97,31 +97,61 @@ class Request:
     admitted: Optional[float] = None
     done: Optional[float] = None
     result: Optional[dict] = None
+    scenario: Optional[Scenario] = None  # the payload, once built (prepare)
+
+    def prepare(self) -> Scenario:
+        if self.scenario is None:
+            self.scenario = self.make()
+        return self.scenario
+
+    def work(self) -> float:
+        """Work estimate: cells x horizon."""
+        s = self.prepare()
+        return float(s.n_cells) * float(s.t_end)
 
 
 def serve_stream(requests: Sequence[Request], hbm_budget_bytes: int, chunk: int = 8,
                  max_slots: int = 1024, device: int = 0, keep_state: bool = False,
-                 time_scale: float = 1.0) -> dict:
+                 time_scale: float = 1.0, policy: str = "fifo",
+                 max_active_cells: Optional[int] = None) -> dict:
     """Run an arrival stream (arrival times in seconds of wall clock, scaled
-    by time_scale) through a server; FIFO admission. Returns per-request
-    latencies and the throughput."""
+    by time_scale) through a server. Admission: "fifo" in arrival order, or
+    "srpt", the arrived request with the least work (cells x horizon) first.
+    max_active_cells caps the cells advancing together (a request is admitted
+    while the cap holds, or when nothing runs); the HBM budget and max_slots
+    always apply. Payloads are built when first needed (Request.prepare; call
+    it beforehand to keep generation out of the served time). Returns
+    per-request latencies and the throughput."""
+    if policy not in ("fifo", "srpt"):
+        raise ValueError("policy must be 'fifo' or 'srpt'")
     pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
+    arrived: List[Request] = []
     by_slot: Dict[int, Request] = {}
-    head: Optional[Scenario] = None
+    active_cells = 0
     with Server(hbm_budget_bytes, max_slots=max_slots, device=device) as srv:
         t0 = time.perf_counter()
         now = lambda: (time.perf_counter() - t0) / time_scale  # noqa: E731
-        while pending or by_slot:
+        while pending or arrived or by_slot:
             while pending and pending[0].arrival <= now():
-                if head is None:
-                    head = pending[0].make()
-                slot = srv.try_admit(head)
+                arrived.append(pending.popleft())
+            if policy == "srpt":
+                arrived.sort(key=lambda r: r.work())
+            while arrived:
+                r = arrived[0]
+                s = r.prepare()
+                if (max_active_cells is not None and by_slot
+                        and active_cells + s.n_cells > max_active_cells):
+                    break
+                slot = srv.try_admit(s)
                 if slot is None:
                     break
-                r = pending.popleft()
+                arrived.pop(0)
                 r.admitted = now()
                 by_slot[slot] = r
-                head = None
+                active_cells += s.n_cells
+            if not by_slot and arrived:
+                raise RuntimeError(f"request {arrived[0].rid} does not fit the server "
+                                   "(HBM budget or slots)")
             if not by_slot:
                 if pending:
                     time.sleep(max(0.0, min(0.01, (pending[0].arrival - now()) * time_scale)))
@@ -130,13 +160,15 @@ def serve_stream(requests: Sequence[Request], hbm_budget_bytes: int, chunk: int 
             for slot in srv.finished():
                 res = srv.collect(slot, with_state=keep_state)
                 r = by_slot.pop(slot)
+                active_cells -= r.scenario.n_cells
                 r.done = now()
                 r.result = res
         makespan = now()
     lat = np.array([r.done - r.arrival for r in requests])
     return {"latency_p50": float(np.percentile(lat, 50)), "latency_p99": float(np.percentile(lat, 99)),
             "solves_per_s": len(requests) / makespan, "makespan": makespan,
-            "n": len(requests), "failed": sum(1 for r in requests if r.result["status"] != 0)}
+            "n": len(requests), "failed": sum(1 for r in requests if r.result["status"] != 0),
+            "latencies": lat.tolist()}
 
 
 def request_stream(count: int, rate: float, seed: int = 0, sides=(128, 256, 512, 1024, 2048),
