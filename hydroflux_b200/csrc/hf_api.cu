@@ -428,13 +428,8 @@ int hf_sim_create(const hf_mesh_desc* mesh, const double* h, const double* hu, c
     return fail(HF_ERR_INVALID_ARG, "dx and dy must be strictly positive");
   HF_TRY(check_bcs(cfg->boundaries, mesh->n_rows, mesh->n_cols));
   const int64_t ncell = mesh->n_rows * mesh->n_cols;
-  if (mesh->manning) {
-    for (int64_t k = 0; k < ncell; ++k)
-      if (!(mesh->manning[k] >= 0.0))
-        return fail(HF_ERR_INVALID_ARG, "Manning n must be non-negative at every cell");
-  } else if (!(mesh->manning_uniform >= 0.0)) {
+  if (!mesh->manning && !(mesh->manning_uniform >= 0.0))
     return fail(HF_ERR_INVALID_ARG, "Manning n must be non-negative");
-  }
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
     cudaGetLastError();
@@ -482,6 +477,18 @@ int hf_sim_create(const hf_mesh_desc* mesh, const double* h, const double* hu, c
   c.check_finite = cfg->check_finite;
   if (cudaMemcpy(s->d_ctrl, &c, sizeof c, cudaMemcpyHostToDevice) != cudaSuccess)
     return done(cuda_fail(cudaGetLastError(), "init ctrl"));
+  if (mesh->manning) {  // n >= 0 at every cell, counted on the device into ctrl.nonfinite
+    unsigned long long bad = 0;
+    if ((rc = launch_count_bad_manning(ncell, s->d_n, &s->d_ctrl->nonfinite, s->stream)) ||
+        cudaMemcpyAsync(&bad, &s->d_ctrl->nonfinite, sizeof bad, cudaMemcpyDeviceToHost,
+                        s->stream) != cudaSuccess ||
+        cudaStreamSynchronize(s->stream) != cudaSuccess)
+      return done(rc ? fail(rc, "Manning check") : cuda_fail(cudaGetLastError(), "Manning check"));
+    if (bad)
+      return done(fail(HF_ERR_INVALID_ARG, "Manning n must be non-negative at every cell"));
+    if (cudaMemcpy(s->d_ctrl, &c, sizeof c, cudaMemcpyHostToDevice) != cudaSuccess)
+      return done(cuda_fail(cudaGetLastError(), "init ctrl"));
+  }
   if ((rc = upload3(s, h, hu, hv)) != HF_OK) return done(rc);
   *out = s;
   return HF_OK;

@@ -150,6 +150,9 @@ int launch_rain(int64_t ncell, double* h, double* hu, double* hv, double rate, d
 int launch_point_sources(int64_t nc, double* h, double* hu, double* hv, int n,
                          const int64_t* rows, const int64_t* cols, const double* q, double dt,
                          double dx, double dy, void* stream);
+// *count += cells with !(n >= 0) (count is device memory, zeroed by the caller).
+int launch_count_bad_manning(int64_t ncell, const double* n, unsigned long long* count,
+                             void* stream);
 int launch_hllc(int x_dir, int64_t n, const double* ul, const double* ur, double* out,
                 void* stream);
 int stage_grid_size(int tiles, int device);

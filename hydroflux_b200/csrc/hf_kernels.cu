@@ -45,6 +45,30 @@ __global__ void __launch_bounds__(NTHREADS, StageOcc<T>::value) k_stage(const St
   }
 }
 
+// The f64 stage of one grid, software-pipelined: while a CTA computes the
+// alpha and update phases of one tile, the raw inputs of its next tile are
+// already being copied into shared memory (cp.async), so the next tile
+// starts without waiting on global memory. Results are those of k_stage.
+__global__ void __launch_bounds__(NTHREADS, HF_MIN_BLOCKS) k_stage_pf(const StageArgs A) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  StagePfSmem& P = *reinterpret_cast<StagePfSmem*>(smem_raw);
+  if (!A.ctrl->active) return;
+  const int ntiles = A.tiles_x * A.tiles_y;
+  double sxm = 0.0, sym = 0.0;
+  unsigned long long nonfin = 0;
+  if ((int)blockIdx.x < ntiles) stage_prefetch(A, P.s, P.hst, blockIdx.x);
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    cp_async_wait_all();
+    __syncthreads();
+    const int next = tile + (int)gridDim.x < ntiles ? tile + (int)gridDim.x : -1;
+    stage_tile<double, true>(A, P.s, tile, sxm, sym, nonfin, P.hst, next);
+  }
+  if (A.finalize) {
+    block_reduce_speeds(sxm, sym, nonfin, A.ctrl);
+    if (blockIdx.x == 0 && threadIdx.x == 0) commit_clock(A.ctrl);
+  }
+}
+
 // One stage of every grid of an ensemble in one launch: the persistent grid
 // walks the concatenated tile list of all scenarios; tile t belongs to
 // scenario tile_scn[t], whose arguments (own sizes, dt, forcings, control
@@ -330,6 +354,18 @@ __global__ void k_point_sources(PointChunk pc, double* h, double* hu, double* hv
   }
 }
 
+// Counts cells whose Manning value is negative or NaN (Mesh2D's requirement
+// n >= 0), checked on the device after the upload.
+__global__ void k_count_bad_manning(int64_t ncell, const double* __restrict__ n,
+                                    unsigned long long* count) {
+  unsigned long long bad = 0;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < ncell;
+       k += (int64_t)gridDim.x * blockDim.x)
+    bad += !(n[k] >= 0.0);
+  for (int o = 16; o > 0; o >>= 1) bad += __shfl_xor_sync(0xffffffffu, bad, o);
+  if ((threadIdx.x & 31) == 0 && bad) atomicAdd(count, bad);
+}
+
 __global__ void k_hllc(int x_dir, int64_t n, const double* ul, const double* ur, double* out) {
   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n;
        k += (int64_t)gridDim.x * blockDim.x) {
@@ -377,12 +413,12 @@ int stage_grid_size(int tiles, int device) {
     per_sm = cached[device];
   } else {
     DevGuard dg(device);
-    cudaFuncSetAttribute(k_stage<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)sizeof(StageSmem));
+    cudaFuncSetAttribute(k_stage_pf, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(StagePfSmem));
     cudaFuncSetAttribute(k_stage_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)sizeof(StageSmem));
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stage<double>, NTHREADS,
-                                                  sizeof(StageSmem));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stage_pf, NTHREADS,
+                                                  sizeof(StagePfSmem));
     if (per_sm < 1) per_sm = 1;
     if (device >= 0 && device < 64) cached[device] = per_sm;
   }
@@ -414,7 +450,7 @@ int stage_dual_grid_size(int tiles, int device) {
 // kernel's dynamic shared-memory limit on this device (never inside a
 // stream capture).
 int launch_stage(const StageArgs& a, int grid, void* stream) {
-  k_stage<double><<<grid, NTHREADS, sizeof(StageSmem), (cudaStream_t)stream>>>(a);
+  k_stage_pf<<<grid, NTHREADS, sizeof(StagePfSmem), (cudaStream_t)stream>>>(a);
   return cuda_rc(cudaGetLastError());
 }
 
@@ -518,6 +554,13 @@ int launch_point_sources(int64_t nc, double* h, double* hu, double* hv, int n,
     if (rc) return rc;
   }
   return 0;
+}
+
+int launch_count_bad_manning(int64_t ncell, const double* n, unsigned long long* count,
+                             void* stream) {
+  if (ncell <= 0) return 0;
+  k_count_bad_manning<<<elem_grid(ncell), 256, 0, (cudaStream_t)stream>>>(ncell, n, count);
+  return cuda_rc(cudaGetLastError());
 }
 
 int launch_hllc(int x_dir, int64_t n, const double* ul, const double* ur, double* out,

@@ -133,13 +133,63 @@ __device__ __forceinline__ void commit_clock(Ctrl* c) {
 
 }  // namespace
 
+// 8-byte asynchronous global -> shared copy; `valid` false zero-fills the
+// destination without reading `gmem` (which must still be a valid address).
+__device__ __forceinline__ void cp_async8(double* smem, const double* gmem, bool valid) {
+  const unsigned saddr = (unsigned)__cvta_generic_to_shared(smem);
+  const int bytes = valid ? 8 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(saddr), "l"(gmem),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
+// Shared memory of the pipelined f64 stage: the tile plus a staging buffer
+// for the next tile's depth (its z, hu and hv are staged in eta, u and v,
+// which are dead once the faces are done).
+struct StagePfSmem {
+  StageSmem s;
+  double hst[R4N];
+};
+
+// Starts the copies of a tile's raw inputs: h (4-cell halo) into hst and z,
+// hu, hv (3-cell halo) into S.eta, S.u, S.v; cells outside the grid read as
+// zeros. Completed by cp_async_wait_all() and a barrier.
+__device__ __forceinline__ void stage_prefetch(const StageArgs& A, StageSmem& S, double* hst,
+                                               int tile) {
+  const int nr = A.nr, nc = A.nc;
+  const int tyi = tile / A.tiles_x;
+  const int gi0 = tyi * TY, gj0 = (tile - tyi * A.tiles_x) * TX;
+  for (int k = threadIdx.x; k < R4N; k += NTHREADS) {
+    const int r = k / R4W, cc = k - r * R4W;
+    const int gi = gi0 + r - 4, gj = gj0 + cc - 4;
+    const bool real = gi >= 0 && gi < nr && gj >= 0 && gj < nc;
+    const int64_t g = real ? (int64_t)gi * nc + gj : 0;
+    cp_async8(&hst[k], A.in_h + g, real);
+    if (r >= 1 && r < R4H - 1 && cc >= 1 && cc < R4W - 1) {
+      const int k3 = (r - 1) * R3W + (cc - 1);
+      cp_async8(&S.eta[k3], A.z + g, real);
+      cp_async8(&S.u[k3], A.in_hu + g, real);
+      cp_async8(&S.v[k3], A.in_hv + g, real);
+    }
+  }
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+
 // Phases 1-4 of one forward-Euler stage (update.rs:805-1053) on one tile:
 // depth snapshot, primitives, limited slopes, face fluxes and the alpha
 // rescaling factors of the tile and its one-cell ring, all in shared memory.
 // Called by every thread of the CTA; ends with a barrier.
-template <class T>
+// With PF (f64 only) the tile's raw inputs are already in shared memory
+// (stage_prefetch into hst, S.eta, S.u, S.v, completed by the caller), and
+// once the faces are done the copies of tile `next` (if >= 0) are started,
+// overlapping the alpha and update phases of this tile.
+template <class T, bool PF = false>
 __device__ __forceinline__ void stage_tile_faces(const StageArgs& A, StageSmemT<T>& S, int gi0,
-                                                 int gj0, double dt) {
+                                                 int gj0, double dt, double* hst = nullptr,
+                                                 int next = -1) {
   const int nr = A.nr, nc = A.nc;
   const double dx = A.dx, dy = A.dy;
   const double dt_dx = dt / dx;  // update.rs:930-931
@@ -147,7 +197,29 @@ __device__ __forceinline__ void stage_tile_faces(const StageArgs& A, StageSmemT<
   const double half_dx = 0.5 * dx, half_dy = 0.5 * dy;
   const int tid = threadIdx.x;
   const T Z = cst<T>(0.0);
-  {
+  if constexpr (PF) {
+    // ---- depth snapshot and primitives from the staged inputs. Cells outside
+    // the grid were zero-filled, so they get h = z = eta = u = v = +0 as below.
+    for (int k = tid; k < R4N; k += NTHREADS) {
+      const int r = k / R4W, cc = k - r * R4W;
+      const double hh = hst[k];
+      S.h[k] = hh;
+      if (r >= 1 && r < R4H - 1 && cc >= 1 && cc < R4W - 1) {
+        const int k3 = (r - 1) * R3W + (cc - 1);
+        const double zz = S.eta[k3], qu = S.u[k3], qv = S.v[k3];
+        double uu = 0.0, vv = 0.0;
+        if (hh > H_VEL) {
+          uu = hfa::div_rn(qu, hh);
+          vv = hfa::div_rn(qv, hh);
+        }
+        S.z[k3] = zz;
+        S.eta[k3] = hh + zz;
+        S.u[k3] = uu;
+        S.v[k3] = vv;
+      }
+    }
+    __syncthreads();
+  } else {
     // ---- depth snapshot (halo 4) and primitives (halo 3): update.rs:853-858, 405-426
     for (int k = tid; k < R4N; k += NTHREADS) {
       const int r = k / R4W, cc = k - r * R4W;
@@ -175,7 +247,8 @@ __device__ __forceinline__ void stage_tile_faces(const StageArgs& A, StageSmemT<
       }
     }
     __syncthreads();
-
+  }
+  {
     // ---- limited slopes: update.rs:459-540
     for (int k = tid; k < SXN + SYN; k += NTHREADS) {
       const bool xd = k < SXN;
@@ -325,6 +398,9 @@ __device__ __forceinline__ void stage_tile_faces(const StageArgs& A, StageSmemT<
       }
     }
     __syncthreads();
+    if constexpr (PF) {
+      if (next >= 0) stage_prefetch(A, S, hst, next);  // eta, u, v and hst are dead now
+    }
 
     // ---- alpha mass rescaling factors: update.rs:953-982 (tile + 1-cell ring)
     for (int k = tid; k < AN; k += NTHREADS) {
@@ -374,9 +450,10 @@ __device__ __forceinline__ void cell_face_beds(const StageArgs& A, const double*
 // One forward-Euler stage (update.rs:805-1211) on one tile of one grid. Called
 // by every thread of the CTA; accumulates the CTA's CFL maxima for the
 // finalize epilogue into (sxm, sym, nonfin).
-template <class T>
+template <class T, bool PF = false>
 __device__ __forceinline__ void stage_tile(const StageArgs& A, StageSmemT<T>& S, int tile,
-                                           double& sxm, double& sym, unsigned long long& nonfin) {
+                                           double& sxm, double& sym, unsigned long long& nonfin,
+                                           double* hst = nullptr, int next = -1) {
   Ctrl* ctrl = A.ctrl;
   const double dt = ctrl->dt;
   const int nr = A.nr, nc = A.nc;
@@ -388,7 +465,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, StageSmemT<T>& S,
   {
     const int tyi = tile / A.tiles_x;
     const int gi0 = tyi * TY, gj0 = (tile - tyi * A.tiles_x) * TX;
-    stage_tile_faces<T>(A, S, gi0, gj0, dt);
+    stage_tile_faces<T, PF>(A, S, gi0, gj0, dt, hst, next);
 
     // ---- FV update + bed source + floor: update.rs:1071-1210
     int src_lo = 0, src_hi = 0;

@@ -173,7 +173,7 @@ class Mesh2D:
             if manning.shape != bed.shape:
                 raise ValueError(f"manning field shape {manning.shape} must match bed shape "
                                  f"{bed.shape}")
-            if not np.all(manning >= 0.0):
+            if not manning.min() >= 0.0:  # a NaN minimum fails too
                 raise ValueError("Manning n must be non-negative at every cell")
         self.bed, self.dx, self.dy, self.manning = bed, float(dx), float(dy), manning
 

@@ -260,6 +260,20 @@ def test_simulation_step_and_errors(gpu, oracle):
         sim.Simulation(mesh, (h0, zeros, zeros), sim.SimulationConfig(cfl=1.5))
     with pytest.raises(sim.ShapeMismatch):
         sim.Simulation(mesh, (h0[:4], zeros, zeros))
+    # The C ABI checks the Manning field itself (on the device after upload).
+    import ctypes as C
+
+    from hydroflux_b200._lib import lib
+    dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))  # noqa: E731
+    for bad in (-0.01, np.nan):
+        n = np.full_like(z, 0.03)
+        n[3, 5] = bad
+        desc = abi.hf_mesh_desc(8, 8, 1.0, 1.0, dp(z), dp(n), 0.0)
+        cfg = abi.make_config()
+        hnd = C.c_void_p()
+        rc = lib().hf_sim_create(C.byref(desc), dp(h0), dp(zeros), dp(zeros), C.byref(cfg), 0,
+                                 C.byref(hnd))
+        assert rc == abi.HF_ERR_INVALID_ARG and not hnd.value
 
 
 def test_driver_matches_hand_loop_bitwise(gpu):
