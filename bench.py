@@ -290,7 +290,7 @@ def run_ours(a, d: Dist):
         "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
                      "frac": achieved_gbs / peak, "peak_source": peak_kind,
                      "traffic": (traffic_per_cell * cells) if traffic_per_cell else None,
-                     "kernel": "k_stage", "alg_bytes_per_launch": bytes_per_launch,
+                     "kernel": "k_stage_pf", "alg_bytes_per_launch": bytes_per_launch,
                      "avg_launch_ms": avg_stage_s * 1e3, "launches": stage_launches},
         "cpu_baseline": cpu,
         "clocks": clk,
