@@ -70,6 +70,12 @@ PROTOTYPES = {
     "hf_grad_manning": (C.c_int, [_VP, _D, _D, _D, _D, _D, _D]),
     "hf_calib_final_state": (C.c_int, [_VP, _D, _D, _D, _D, _D, _D]),
     "hf_calib_dt": (C.c_int, [_VP, _D, C.POINTER(C.c_int64)]),
+    "hf_read_ascii_grid": (C.c_int, [C.c_char_p, C.POINTER(abi.hf_ascii_grid_header),
+                                     C.POINTER(_D)]),
+    "hf_free_buffer": (None, [_VP]),
+    "hf_write_ascii_grid": (C.c_int, [C.c_char_p, C.POINTER(abi.hf_ascii_grid_header), _D]),
+    "hf_depth_raster": (C.c_int, [C.c_int64, _D, C.c_int, C.c_double, _D]),
+    "hf_worldcover_manning": (C.c_double, [C.c_int]),
     "hf_workspace_create": (C.c_int, [C.c_int64, C.c_int64, C.c_int, C.POINTER(_VP)]),
     "hf_workspace_destroy": (C.c_int, [_VP]),
     "hf_cfl_time_step": (C.c_int, [C.POINTER(abi.hf_grid), _VP, _VP, _VP,

@@ -86,3 +86,8 @@ def make_config(cfl=0.4, integrator=HF_SSPRK2, boundaries=None, max_steps=10_000
         boundaries = make_boundaries(w, w, w, w)
     return hf_config(float(cfl), int(integrator), int(check_finite), boundaries,
                      int(max_steps), float(max_dt), float(friction_dry_tol))
+
+
+class hf_ascii_grid_header(C.Structure):
+    _fields_ = [("ncols", C.c_int64), ("nrows", C.c_int64), ("xllcorner", C.c_double),
+                ("yllcorner", C.c_double), ("cellsize", C.c_double), ("nodata_value", C.c_double)]

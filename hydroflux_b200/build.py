@@ -18,7 +18,7 @@ INCLUDE = os.path.join(ROOT, "include")
 OUT = os.path.join(HERE, "libhydroflux_gpu.so")
 
 SOURCES = ["hf_kernels.cu", "hf_api.cu", "hf_noalloc.cu", "hf_batch.cu", "hf_serve.cu",
-           "hf_adjoint.cu", "hf_calib.cu"]
+           "hf_adjoint.cu", "hf_calib.cu", "hf_io.cu"]
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-prec-div=true",
               "-prec-sqrt=true", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
@@ -61,7 +61,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         subprocess.run(cmd, check=True)
         objs.append(obj)
     tmp = OUT + ".tmp"
-    subprocess.run([nvcc(), *GENCODE, "-shared", "-cudart", "static", "-o", tmp, *objs],
+    subprocess.run([nvcc(), *GENCODE, "-shared", "-cudart", "static", "-o", tmp, *objs, "-lz"],
                    check=True)
     os.replace(tmp, OUT)
     return OUT

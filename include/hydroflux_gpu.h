@@ -301,6 +301,39 @@ int hf_calib_final_state(hf_calib* calib, double* h, double* hu, double* hv, dou
 int hf_calib_dt(hf_calib* calib, double* dts, int64_t* n);
 
 /* ---------------------------------------------------------------------------
+ * Rasters on the host: ESRI ASCII grids (solver-2d/src/ascii_grid.rs) and the
+ * depth raster / land-cover roughness helpers of solver-2d/src/io.rs.
+ * ------------------------------------------------------------------------- */
+typedef struct hf_ascii_grid_header {
+  int64_t ncols;
+  int64_t nrows;
+  double xllcorner;     /* south-west corner of the grid */
+  double yllcorner;
+  double cellsize;
+  double nodata_value;
+} hf_ascii_grid_header;
+
+/* read_ascii_grid (ascii_grid.rs:101-160): the six header lines in order
+ * (ncols, nrows, xllcorner, yllcorner, cellsize, NODATA_value; keys matched
+ * case-insensitively), then exactly ncols * nrows numbers in any line layout,
+ * row 0 = the first data row (north). A path ending in ".gz" is gunzipped.
+ * *data receives a malloc'd row-major array (free with hf_free_buffer).
+ * Errors: HF_ERR_INVALID_ARG (I/O, header, unparsable value),
+ * HF_ERR_SHAPE_MISMATCH (value count). */
+int hf_read_ascii_grid(const char* path, hf_ascii_grid_header* header, double** data);
+void hf_free_buffer(void* p);
+/* Writes an ESRI ASCII grid (gzip when the path ends in ".gz") whose values
+ * hf_read_ascii_grid returns bit for bit (%.17g). No counterpart in the
+ * reference, which writes GeoTIFF through surtgis. */
+int hf_write_ascii_grid(const char* path, const hf_ascii_grid_header* header, const double* data);
+/* depth_raster_from_states (io.rs:216-234): out[k] = h[k], or nodata where
+ * h[k] <= H_DRY when use_nodata != 0. */
+int hf_depth_raster(int64_t ncell, const double* h, int use_nodata, double nodata, double* out);
+/* esa_worldcover_to_manning (io.rs:192-207): Manning n of an ESA WorldCover
+ * land-cover class (0.040 for unlisted codes). */
+double hf_worldcover_manning(int code);
+
+/* ---------------------------------------------------------------------------
  * Low-level entry points on caller-owned device buffers, mirroring the
  * reference's free functions. All run on `stream` and are asynchronous
  * unless they return a host value (hf_cfl_time_step synchronizes it).
