@@ -46,6 +46,11 @@ PROTOTYPES = {
                                       C.POINTER(_VP)]),
     "hf_sim_set_rain": (C.c_int, [_VP, C.c_int64, _D, _D]),
     "hf_sim_set_point_sources": (C.c_int, [_VP, C.c_int64, _I64P, _I64P, _I64P, _D, _D]),
+    "hf_sim_set_rain_units": (C.c_int, [_VP, C.c_double, C.c_double, C.c_double]),
+    "hf_sim_set_point_source_units": (C.c_int, [_VP, C.c_double, C.c_double, C.c_double]),
+    "hf_sim_set_gauges": (C.c_int, [_VP, C.c_int64, _I64P, _I64P, C.c_int64]),
+    "hf_sim_gauge_peaks": (C.c_int, [_VP, _D, _D]),
+    "hf_sim_gauge_series": (C.c_int, [_VP, _D, _D, _I64P, _I64P]),
     "hf_batch_create": (C.c_int, [C.c_int64, C.POINTER(abi.hf_scenario_desc), C.c_int,
                                   C.POINTER(_VP)]),
     "hf_batch_destroy": (C.c_int, [_VP]),

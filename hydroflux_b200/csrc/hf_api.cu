@@ -141,6 +141,8 @@ ForcingDev ForcingHost::dev() const {
   f.tile_start = d_tile_start;
   f.tile_order = d_tile_order;
   f.src_dh = d_dh;
+  f.rain_u = rain_u;
+  f.src_u = src_u;
   return f;
 }
 
@@ -224,6 +226,7 @@ struct hf_sim {
   Ctrl* d_ctrl = nullptr;
   Ctrl* h_ctrl = nullptr;  // pinned mirror
   ForcingHost forcing;
+  GaugeDev gauge{};  // n == 0: no gauges
   cudaGraphExec_t graphs[3] = {nullptr, nullptr, nullptr};
   bool cfl_dirty = true;
   double last_dt = 0.0;
@@ -276,7 +279,16 @@ int enqueue_step(hf_sim* s) {
     HF_TRY(launch_stage(stage_args(s, true), s->grid, s->stream));
   else
     HF_TRY(launch_finalize(stage_args(s, true), s->grid, s->stream));
+  if (s->gauge.n > 0) HF_TRY(launch_gauges(s->d_ctrl, s->d_h, s->gauge, 0, s->stream));
   return HF_OK;
+}
+
+void release_gauges(hf_sim* s) {
+  GaugeDev& g = s->gauge;
+  for (void* p : {(void*)g.cell, (void*)g.peak, (void*)g.last, (void*)g.ser_t, (void*)g.ser_h,
+                  (void*)g.count})
+    dfree(p);
+  g = GaugeDev{};
 }
 
 void drop_graphs(hf_sim* s) {
@@ -382,6 +394,7 @@ void destroy_sim(hf_sim* s) {
   drop_graphs(s);
   s->forcing.release_rain();
   s->forcing.release_src();
+  release_gauges(s);
   for (void* p : {(void*)s->d_z, (void*)s->d_n, (void*)s->d_h, (void*)s->d_hu, (void*)s->d_hv,
                   (void*)s->d_h1, (void*)s->d_hu1, (void*)s->d_hv1, (void*)s->d_ctrl})
     dfree(p);
@@ -604,6 +617,8 @@ int hf_sim_run_steps_timed(hf_sim* s, uint64_t n_steps, double t_target, double*
     rc = ssp ? launch_stage(stage_args(s, true), s->grid, s->stream)
              : launch_finalize(stage_args(s, true), s->grid, s->stream);
     cudaEventRecord(ev[3 * k + 2], s->stream);
+    if (rc == HF_OK && s->gauge.n > 0)
+      rc = launch_gauges(s->d_ctrl, s->d_h, s->gauge, 0, s->stream);
   }
   if (rc == HF_OK) rc = read_ctrl(s);
   if (rc == HF_OK) {
@@ -732,6 +747,106 @@ int hf_sim_set_point_sources(hf_sim* s, int64_t n_sources, const int64_t* rows,
   drop_graphs(s);
   return forcing_set_sources(s->forcing, s->nr, s->nc, s->tiles_x, s->tiles_y, n_sources, rows,
                              cols, offsets, t, q);
+}
+
+int hf_sim_set_rain_units(hf_sim* s, double t_div, double v_mul, double v_div) {
+  if (!s) return fail(HF_ERR_INVALID_ARG, "null handle");
+  if (!(std::isfinite(t_div) && t_div > 0.0 && std::isfinite(v_mul) && std::isfinite(v_div) &&
+        v_div != 0.0))
+    return fail(HF_ERR_INVALID_ARG, "series units: t_div must be finite and > 0, v_mul finite, "
+                                    "v_div finite and non-zero");
+  DeviceGuard guard(s->device);
+  cudaStreamSynchronize(s->stream);
+  drop_graphs(s);
+  s->forcing.rain_u = SeriesUnits{t_div, v_mul, v_div};
+  return HF_OK;
+}
+
+int hf_sim_set_point_source_units(hf_sim* s, double t_div, double v_mul, double v_div) {
+  if (!s) return fail(HF_ERR_INVALID_ARG, "null handle");
+  if (!(std::isfinite(t_div) && t_div > 0.0 && std::isfinite(v_mul) && std::isfinite(v_div) &&
+        v_div != 0.0))
+    return fail(HF_ERR_INVALID_ARG, "series units: t_div must be finite and > 0, v_mul finite, "
+                                    "v_div finite and non-zero");
+  DeviceGuard guard(s->device);
+  cudaStreamSynchronize(s->stream);
+  drop_graphs(s);
+  s->forcing.src_u = SeriesUnits{t_div, v_mul, v_div};
+  return HF_OK;
+}
+
+int hf_sim_set_gauges(hf_sim* s, int64_t n_gauges, const int64_t* rows, const int64_t* cols,
+                      int64_t capacity) {
+  if (!s) return fail(HF_ERR_INVALID_ARG, "null handle");
+  if (n_gauges < 0 || n_gauges > (1 << 20) || capacity < 0 ||
+      (n_gauges > 0 && (!rows || !cols)))
+    return fail(HF_ERR_INVALID_ARG, "bad gauge arguments");
+  if (n_gauges > 0 && capacity > (int64_t)(((size_t)1 << 40) / (size_t)(n_gauges + 1)))
+    return fail(HF_ERR_INVALID_ARG, "gauge capacity too large");
+  std::vector<long long> cell((size_t)n_gauges);
+  for (int64_t k = 0; k < n_gauges; ++k) {
+    if (rows[k] < 0 || rows[k] >= s->nr || cols[k] < 0 || cols[k] >= s->nc)
+      return fail(HF_ERR_INVALID_ARG, "gauge " + std::to_string(k) + " (" +
+                                          std::to_string(rows[k]) + ", " +
+                                          std::to_string(cols[k]) + ") is outside the grid");
+    cell[(size_t)k] = (long long)(rows[k] * s->nc + cols[k]);
+  }
+  DeviceGuard guard(s->device);
+  cudaStreamSynchronize(s->stream);
+  drop_graphs(s);
+  release_gauges(s);
+  if (n_gauges == 0) return HF_OK;
+  GaugeDev g{};
+  const size_t n = (size_t)n_gauges, cap = (size_t)capacity;
+  int rc = dalloc((long long**)&g.cell, n);
+  if (!rc) rc = dalloc(&g.peak, n);
+  if (!rc) rc = dalloc(&g.last, n);
+  if (!rc) rc = dalloc(&g.ser_t, std::max<size_t>(cap, 1));
+  if (!rc) rc = dalloc(&g.ser_h, std::max<size_t>(cap * n, 1));
+  if (!rc) rc = dalloc(&g.count, 1);
+  g.n = (int)n_gauges;
+  g.cap = (long long)capacity;
+  s->gauge = g;
+  if (rc) {
+    release_gauges(s);
+    return rc;
+  }
+  HF_CUDA(cudaMemcpyAsync((void*)g.cell, cell.data(), n * sizeof(long long),
+                          cudaMemcpyHostToDevice, s->stream));
+  HF_CUDA(cudaMemsetAsync(g.count, 0, sizeof(long long), s->stream));
+  HF_TRY(launch_gauges(s->d_ctrl, s->d_h, s->gauge, 1, s->stream));
+  HF_CUDA(cudaStreamSynchronize(s->stream));
+  return HF_OK;
+}
+
+int hf_sim_gauge_peaks(hf_sim* s, double* peak, double* last) {
+  if (!s) return fail(HF_ERR_INVALID_ARG, "null handle");
+  if (s->gauge.n == 0) return fail(HF_ERR_INVALID_ARG, "no gauges set");
+  DeviceGuard guard(s->device);
+  HF_CUDA(cudaStreamSynchronize(s->stream));
+  const size_t bytes = (size_t)s->gauge.n * sizeof(double);
+  if (peak) HF_CUDA(cudaMemcpy(peak, s->gauge.peak, bytes, cudaMemcpyDeviceToHost));
+  if (last) HF_CUDA(cudaMemcpy(last, s->gauge.last, bytes, cudaMemcpyDeviceToHost));
+  return HF_OK;
+}
+
+int hf_sim_gauge_series(hf_sim* s, double* t, double* h, int64_t* n_stored, int64_t* n_seen) {
+  if (!s) return fail(HF_ERR_INVALID_ARG, "null handle");
+  if (s->gauge.n == 0) return fail(HF_ERR_INVALID_ARG, "no gauges set");
+  DeviceGuard guard(s->device);
+  HF_CUDA(cudaStreamSynchronize(s->stream));
+  long long count = 0;
+  HF_CUDA(cudaMemcpy(&count, s->gauge.count, sizeof count, cudaMemcpyDeviceToHost));
+  const long long stored = std::min(count, s->gauge.cap);
+  if (n_stored) *n_stored = stored;
+  if (n_seen) *n_seen = count;
+  if (stored > 0 && t)
+    HF_CUDA(cudaMemcpy(t, s->gauge.ser_t, (size_t)stored * sizeof(double),
+                       cudaMemcpyDeviceToHost));
+  if (stored > 0 && h)
+    HF_CUDA(cudaMemcpy(h, s->gauge.ser_h, (size_t)stored * s->gauge.n * sizeof(double),
+                       cudaMemcpyDeviceToHost));
+  return HF_OK;
 }
 
 // ------------------------------------------------------------ workspace

@@ -235,6 +235,16 @@ __device__ __forceinline__ double series_eval(const double* ts, const double* vs
   return vs[lo] + (vs[lo + 1] - vs[lo]) * w;
 }
 
+// A series with units: sampled at t / t_div, value (v * v_mul) / v_div, the
+// arithmetic of a caller that keeps its hydrograph in minutes and mm/h
+// (solver-2d/examples/uk_ea_test8a_official.rs:119-134). The default units
+// (1, 1, 1) give series_eval exactly.
+__device__ __forceinline__ double series_eval_u(const double* ts, const double* vs, int n,
+                                                double t, const SeriesUnits& u) {
+  const double v = series_eval(ts, vs, n, hfa::div_rn(t, u.t_div));
+  return hfa::div_rn(v * u.v_mul, u.v_div);
+}
+
 // Wave speeds of an interior cell for the CFL bound (update.rs:121-135).
 __device__ __forceinline__ void cell_speeds(double h, double hu, double hv, double& sx,
                                             double& sy) {

@@ -73,6 +73,12 @@ struct Ctrl {
   long long replay_n;
 };
 
+struct SeriesUnits {
+  double t_div = 1.0;
+  double v_mul = 1.0;
+  double v_div = 1.0;
+};
+
 // Forcing tables on the device (piecewise-linear series). Point sources are
 // bucketed by stage tile: sources of tile t are tile_order[tile_start[t] ..
 // tile_start[t+1]) in their original order.
@@ -89,6 +95,24 @@ struct ForcingDev {
   const int* tile_start;
   const int* tile_order;
   double* src_dh;  // per source, set each step by the control kernel
+  // Series units: a series is sampled at t / t_div and its value converted
+  // as (v * v_mul) / v_div (identity by default; see hf_sim_set_rain_units).
+  SeriesUnits rain_u;
+  SeriesUnits src_u;
+};
+
+// Control-point (gauge) recorder of a simulation: after every step taken,
+// the depth at each gauge cell is folded into its running maximum and stored
+// as one row of the series while rows remain.
+struct GaugeDev {
+  int n;
+  const long long* cell;  // row-major cell index of each gauge
+  double* peak;           // fold(0.0, f64::max) over the recorded depths
+  double* last;
+  double* ser_t;          // cap rows: time of the row
+  double* ser_h;          // cap x n depths
+  long long cap;
+  long long* count;       // rows seen (stored: min(count, cap))
 };
 
 // Tangent arrays of a DualD (forward-mode) stage, parallel to the value
@@ -137,6 +161,9 @@ struct StageArgs {
 int launch_stage(const StageArgs& a, int grid, void* stream);
 int launch_finalize(const StageArgs& a, int grid, void* stream);
 int launch_control(Ctrl* ctrl, double dx, double dy, const ForcingDev& f, void* stream);
+// Records one gauge row when the step ran (init: unconditionally, the peak
+// starting from 0).
+int launch_gauges(const Ctrl* ctrl, const double* h, const GaugeDev& g, int init, void* stream);
 int launch_cfl(const StageArgs& a, int with_ghosts, int grid, void* stream);
 int launch_set_fixed(Ctrl* ctrl, double dt, void* stream);
 int launch_set_step(Ctrl* ctrl, double dt_cap, double cfl, double max_dt, int check_finite,
@@ -205,6 +232,7 @@ struct ForcingHost {
   int* d_tile_start = nullptr;
   int* d_tile_order = nullptr;
   double* d_dh = nullptr;
+  SeriesUnits rain_u, src_u;
   void release_rain();
   void release_src();
   ForcingDev dev() const;

@@ -202,7 +202,8 @@ __device__ int control_step(Ctrl* c, double dx, double dy, const ForcingDev& f) 
         } else {
           c->dt = dt;
           c->t_new = c->t + dt;
-          const double rate = f.n_rain > 0 ? series_eval(f.rain_t, f.rain_v, f.n_rain, c->t_new) : 0.0;
+          const double rate =
+              f.n_rain > 0 ? series_eval_u(f.rain_t, f.rain_v, f.n_rain, c->t_new, f.rain_u) : 0.0;
           c->rain_on = rate != 0.0;
           c->rain_dh = rate * dt;
           c->sx_bits = 0ull;
@@ -222,7 +223,7 @@ __device__ int control_step(Ctrl* c, double dx, double dy, const ForcingDev& f) 
 __device__ __forceinline__ void source_increment(const Ctrl* c, double dx, double dy,
                                                  const ForcingDev& f, int k) {
   const int a = f.src_off[k], b = f.src_off[k + 1];
-  const double q = series_eval(f.src_t + a, f.src_q + a, b - a, c->t_new);
+  const double q = series_eval_u(f.src_t + a, f.src_q + a, b - a, c->t_new, f.src_u);
   f.src_dh[k] = q * c->dt / (dx * dy);
 }
 
@@ -232,6 +233,26 @@ __global__ void k_control(Ctrl* c, double dx, double dy, ForcingDev f) {
   __syncthreads();
   if (s_go)
     for (int k = threadIdx.x; k < f.n_src; k += blockDim.x) source_increment(c, dx, dy, f, k);
+}
+
+// Gauge row after a step: the series the reference's urban example keeps at
+// its control points (solver-2d/examples/uk_ea_test8a_official.rs:219-222)
+// and their peaks (fold(0.0, f64::max), ibid. 243-246; fmax ignores NaN as
+// f64::max does).
+__global__ void k_gauges(const Ctrl* c, const double* __restrict__ h, GaugeDev g, int init) {
+  if (!init && !c->active) return;
+  const long long row = *g.count;
+  for (int k = threadIdx.x; k < g.n; k += blockDim.x) {
+    const double v = h[g.cell[k]];
+    g.peak[k] = fmax(init ? 0.0 : g.peak[k], v);
+    g.last[k] = v;
+    if (row < g.cap) g.ser_h[row * g.n + k] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (row < g.cap) g.ser_t[row] = c->t;
+    *g.count = row + 1;
+  }
 }
 
 // Per-scenario control of an ensemble: one thread per scenario.
@@ -502,6 +523,11 @@ int launch_cfl(const StageArgs& a, int with_ghosts, int grid, void* stream) {
 
 int launch_control(Ctrl* ctrl, double dx, double dy, const ForcingDev& f, void* stream) {
   k_control<<<1, 256, 0, (cudaStream_t)stream>>>(ctrl, dx, dy, f);
+  return cuda_rc(cudaGetLastError());
+}
+
+int launch_gauges(const Ctrl* ctrl, const double* h, const GaugeDev& g, int init, void* stream) {
+  k_gauges<<<1, 128, 0, (cudaStream_t)stream>>>(ctrl, h, g, init);
   return cuda_rc(cudaGetLastError());
 }
 

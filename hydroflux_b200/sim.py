@@ -12,7 +12,7 @@ from __future__ import annotations
 import ctypes as C
 import enum
 from dataclasses import dataclass, field
-from typing import Optional, Sequence
+from typing import Optional, Sequence, Tuple
 
 import numpy as np
 
@@ -355,6 +355,52 @@ class Simulation:
         raise_for(lib().hf_sim_set_point_sources(
             self._h, len(sources), rows.ctypes.data_as(i64), cols.ctypes.data_as(i64),
             offs.ctypes.data_as(i64), _f64p(t), _f64p(q)))
+
+    def set_rain_units(self, t_div: float = 1.0, v_mul: float = 1.0, v_div: float = 1.0) -> None:
+        """The rain series is sampled at t / t_div and its value converted
+        as (v * v_mul) / v_div: (60, 1e-3, 3600) for a hyetograph in minutes
+        and mm/h, with the arithmetic of the reference's urban example
+        (solver-2d/examples/uk_ea_test8a_official.rs:119-129)."""
+        raise_for(lib().hf_sim_set_rain_units(self._h, float(t_div), float(v_mul), float(v_div)))
+
+    def set_point_source_units(self, t_div: float = 1.0, v_mul: float = 1.0,
+                               v_div: float = 1.0) -> None:
+        """Units of every point-source series, as set_rain_units (the
+        example's inflow: t_div = 60, v_mul = cellsize, ibid. 131-134)."""
+        raise_for(lib().hf_sim_set_point_source_units(self._h, float(t_div), float(v_mul),
+                                                      float(v_div)))
+
+    def set_gauges(self, cells: Sequence[Tuple[int, int]], capacity: int = 1 << 20) -> None:
+        """Record the depth at these (row, col) cells after every step, on
+        the device: the control-point series and peaks the reference's
+        urban example keeps (uk_ea_test8a_official.rs:187-246). Row 0 is the
+        current state; at most `capacity` rows are stored."""
+        cells = list(cells)
+        rows = np.array([c[0] for c in cells] or [0], dtype=np.int64)
+        cols = np.array([c[1] for c in cells] or [0], dtype=np.int64)
+        i64 = C.POINTER(C.c_int64)
+        raise_for(lib().hf_sim_set_gauges(self._h, len(cells), rows.ctypes.data_as(i64),
+                                          cols.ctypes.data_as(i64), int(capacity)))
+        self._n_gauges = len(cells)
+
+    def gauge_peaks(self):
+        """(peak, last) depth per gauge; peak = fold(0.0, f64::max) over
+        every recorded depth."""
+        n = getattr(self, "_n_gauges", 0)
+        peak, last = np.empty(max(n, 1)), np.empty(max(n, 1))
+        raise_for(lib().hf_sim_gauge_peaks(self._h, _f64p(peak), _f64p(last)))
+        return peak[:n], last[:n]
+
+    def gauge_series(self):
+        """(t[rows], h[rows, gauges], rows seen): the stored rows."""
+        n = getattr(self, "_n_gauges", 0)
+        stored, seen = C.c_int64(), C.c_int64()
+        raise_for(lib().hf_sim_gauge_series(self._h, None, None, C.byref(stored), C.byref(seen)))
+        t = np.empty(max(stored.value, 1))
+        h = np.empty((max(stored.value, 1), max(n, 1)))
+        raise_for(lib().hf_sim_gauge_series(self._h, _f64p(t), _f64p(h), C.byref(stored),
+                                            C.byref(seen)))
+        return t[:stored.value], h[:stored.value, :n], seen.value
 
     def device_state(self):
         """Zero-copy torch views (h, hu, hv) of the resident state and the

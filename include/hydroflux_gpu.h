@@ -173,6 +173,23 @@ int hf_sim_set_rain(hf_sim* sim, int64_t n_points, const double* t, const double
 int hf_sim_set_point_sources(hf_sim* sim, int64_t n_sources, const int64_t* rows,
                              const int64_t* cols, const int64_t* offsets, const double* t,
                              const double* q);
+/* Units of the rain / point-source series: the series is sampled at
+ * t / t_div and its value converted as (v * v_mul) / v_div, the arithmetic of
+ * a caller that keeps a hyetograph in minutes and mm/h
+ * (uk_ea_test8a_official.rs:119-134: t_div = 60, v_mul = 1e-3, v_div = 3600;
+ * its inflow: v_mul = cellsize). Default (1, 1, 1) is the identity. */
+int hf_sim_set_rain_units(hf_sim* sim, double t_div, double v_mul, double v_div);
+int hf_sim_set_point_source_units(hf_sim* sim, double t_div, double v_mul, double v_div);
+/* Control points (gauges): after every step the depth at each gauge cell is
+ * recorded (the series and fold(0.0, f64::max) peaks the reference's urban
+ * example keeps, uk_ea_test8a_official.rs:187-246). Row 0 is the current
+ * state; rows beyond `capacity` are counted but not stored. n_gauges = 0
+ * clears. */
+int hf_sim_set_gauges(hf_sim* sim, int64_t n_gauges, const int64_t* rows, const int64_t* cols,
+                      int64_t capacity);
+int hf_sim_gauge_peaks(hf_sim* sim, double* peak, double* last);
+/* t: n_stored times; h: n_stored x n_gauges depths (either may be NULL). */
+int hf_sim_gauge_series(hf_sim* sim, double* t, double* h, int64_t* n_stored, int64_t* n_seen);
 
 /* ---------------------------------------------------------------------------
  * Ensembles: many independent scenarios (different grid sizes, beds,

@@ -75,6 +75,20 @@ int check_bcs(const Boundaries& b, int64_t nr, int64_t nc) {
   return HF_OK;
 }
 
+// Units of the forcing series (hf_sim_set_rain_units /
+// hf_sim_set_point_source_units): sampled at t / t_div, value
+// (v * v_mul) / v_div, the order of the reference example's
+// `interp_min(table, t_s) * 1e-3 / 3600.0` (t_s / 60 inside interp_min;
+// solver-2d/examples/uk_ea_test8a_official.rs:119-134).
+struct Units {
+  double t_div = 1.0, v_mul = 1.0, v_div = 1.0;
+};
+Units g_rain_units, g_src_units;  // set by hfo_set_series_units
+
+double series_eval_u(const double* ts, const double* vs, int64_t n, double t, const Units& u) {
+  return series_eval(ts, vs, n, t / u.t_div) * u.v_mul / u.v_div;
+}
+
 // Forcing descriptor (see hf_sim_set_rain / hf_sim_set_point_sources).
 struct Forcing {
   int64_t n_rain = 0;
@@ -86,6 +100,8 @@ struct Forcing {
   const int64_t* offs = nullptr;
   const double* src_t = nullptr;
   const double* src_q = nullptr;
+  Units rain_u = g_rain_units;
+  Units src_u = g_src_units;
 };
 
 // Simulation::step (sim.rs:204-228) followed by the forcings at t_new.
@@ -111,13 +127,14 @@ int sim_step(std::vector<Cons<T>>& st, const Mesh<T>& m, const hf_config& cfg,
   *t += dt;
   *steps += 1;
   const double t_new = *t;
-  if (f.n_rain > 0) apply_rain(st, series_eval(f.rain_t, f.rain_v, f.n_rain, t_new), dt);
+  if (f.n_rain > 0)
+    apply_rain(st, series_eval_u(f.rain_t, f.rain_v, f.n_rain, t_new, f.rain_u), dt);
   if (f.n_src > 0) {
     std::vector<PointSource> ps(f.n_src);
     for (int64_t k = 0; k < f.n_src; ++k) {
       int64_t a = f.offs[k], b = f.offs[k + 1];
       ps[k] = PointSource{f.rows[k], f.cols[k],
-                          series_eval(f.src_t + a, f.src_q + a, b - a, t_new)};
+                          series_eval_u(f.src_t + a, f.src_q + a, b - a, t_new, f.src_u)};
     }
     apply_point_sources(st, m.nc, ps.data(), f.n_src, dt, m.dx, m.dy);
   }
@@ -277,6 +294,12 @@ int hfo_apply_point_sources(int64_t nr, int64_t nc, double* h, double* hu, doubl
 
 double hfo_series_eval(const double* t, const double* v, int64_t n, double x) {
   return series_eval(t, v, n, x);
+}
+
+void hfo_set_series_units(double rain_t_div, double rain_v_mul, double rain_v_div,
+                          double src_t_div, double src_v_mul, double src_v_div) {
+  g_rain_units = Units{rain_t_div, rain_v_mul, rain_v_div};
+  g_src_units = Units{src_t_div, src_v_mul, src_v_div};
 }
 
 // Simulation driver: Simulation::new checks (sim.rs:130-165), then

@@ -38,6 +38,8 @@ def lib():
         _LIB.hfo_series_eval.restype = C.c_double
         _LIB.hfo_pow_cr.restype = C.c_double
         _LIB.hfo_pow_cr.argtypes = [C.c_double, C.c_int]
+        _LIB.hfo_set_series_units.restype = None
+        _LIB.hfo_set_series_units.argtypes = [C.c_double] * 6
     return _LIB
 
 
@@ -183,8 +185,12 @@ class Forcing:
     """Rain series and point-source series (host side of hf_sim_set_rain /
     hf_sim_set_point_sources)."""
 
-    def __init__(self, rain=None, sources=None):
-        # rain: (t array, rate array) or None; sources: list of (row, col, t array, q array)
+    def __init__(self, rain=None, sources=None, rain_units=(1.0, 1.0, 1.0),
+                 src_units=(1.0, 1.0, 1.0)):
+        # rain: (t array, rate array) or None; sources: list of (row, col, t array, q array);
+        # units: (t_div, v_mul, v_div) of each series (hf_sim_set_rain_units)
+        self.rain_units = tuple(float(u) for u in rain_units)
+        self.src_units = tuple(float(u) for u in src_units)
         self.rain_t = _f64(rain[0]) if rain is not None else np.zeros(0)
         self.rain_v = _f64(rain[1]) if rain is not None else np.zeros(0)
         sources = sources or []
@@ -201,6 +207,8 @@ class Forcing:
         self.src_q = np.concatenate(qs) if qs else np.zeros(0)
 
     def args(self):
+        # the units travel through a setter read when the oracle call starts
+        lib().hfo_set_series_units(*self.rain_units, *self.src_units)
         return (C.c_int64(len(self.rain_t)), _p(self.rain_t), _p(self.rain_v),
                 C.c_int64(len(self.rows)), _pi(self.rows), _pi(self.cols), _pi(self.offs),
                 _p(self.src_t), _p(self.src_q))
