@@ -82,7 +82,7 @@ def test_series_units_bitwise(gpu, oracle, integrator):
 
 def test_default_units_are_the_identity(gpu, oracle):
     sim, _ = gpu
-    z, n = urban_like(40, 50, 3)
+    z, n = urban_like(60, 80, 3)
     cfg = sim.SimulationConfig(cfl=0.4, max_dt=2.0)
     out, r = run_pair(sim, oracle, z, n, 2.0, cfg, 150, (1.0, 1.0, 1.0), (1.0, 1.0, 1.0))
     assert exact_fraction(out["state"], (r["h"], r["hu"], r["hv"])) == 1.0
