@@ -49,12 +49,13 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--workload", default="valley", choices=["valley", "ensemble", "adjoint",
-                                                            "serve"],
+                                                            "serve", "lanes"],
                    help="valley: the 4096^2 plain step (default line); ensemble: batched "
                         "uneven-size scenarios vs a loop of per-scenario solves; adjoint: "
                         "misfit gradient w.r.t. the Manning field vs the forward solve; "
                         "serve: an arrival stream through the continuous-batching server vs "
-                        "a sequential plain solve per request")
+                        "a sequential plain solve per request; lanes: zonal Manning "
+                        "derivatives in vector mode vs scalar Dual runs vs the adjoint")
     p.add_argument("--calib-n", type=int, default=512, help="adjoint: grid side")
     p.add_argument("--calib-steps", type=int, default=2000, help="adjoint: steps of the misfit")
     p.add_argument("--checkpoint-every", type=int, default=45)
@@ -249,8 +250,10 @@ def run_ours(a, d: Dist):
         s2.set_rain(np.stack(scn_w.rain, axis=1))
         s2.set_point_sources([S.PointSource(r, c, np.stack([t, q], axis=1))
                               for r, c, t, q in scn_w.sources])
+        t_c = time.perf_counter()
         for _ in range(a.steps):
             s2.step(scn_w.t_end - s2.time())
+        t_s = time.perf_counter()
         from hydroflux_b200._lib import lib as _l
         rc = _l().hf_sim_get_state(s2._h, out[0].data_ptr(), out[1].data_ptr(), out[2].data_ptr())
         assert rc == 0
@@ -261,6 +264,8 @@ def run_ours(a, d: Dist):
         d2h = (3 * cells * 8) / a.steps + 128
         e2e = {"value": d.world * cells * a.steps / el, "unit": UNIT,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "create_ms": 1e3 * (t_c - t_a), "steps_ms": 1e3 * (t_s - t_c),
+               "readback_ms": 1e3 * (t_b - t_s),
                "note": "Simulation::new from pinned host arrays (bed, n, h, hu, hv), K x "
                        "Simulation::step through the C ABI (dt read back each step), "
                        "states() to pinned host; copies, allocation and graph capture timed"}
@@ -535,6 +540,89 @@ def run_adjoint(a, d: Dist):
         print(json.dumps(line), flush=True)
 
 
+def run_lanes(a, d: Dist):
+    """Forward-mode gradients for P zonal Manning parameters (vertical
+    stripes), the trade-off of solver-2d/examples/m1_forward_scaling.rs: P
+    scalar Dual runs (hf_tangent) against one vector-mode run with P lanes
+    (hf_tangent_lanes) and against one reverse sweep (hf_grad_manning), each
+    as a multiple of the forward misfit solve. On the misfit problem of the
+    adjoint line (--calib-n, --calib-steps) and on a 64x64 grid of the same
+    generator, where one Dual grid fills only a tenth of the SMs. Lane
+    derivatives are checked against the zone sums of the adjoint gradient.
+    Replicas on N > 1."""
+    import torch
+
+    from hydroflux_b200 import _lib, calib, workloads
+    dev = d.local
+    torch.cuda.set_device(dev)
+    _lib.lib()
+    counts = (1, 2, 4, 8, 16)
+    by_grid = {}
+    t_all = 0.0
+    clocks = ClockSampler(dev)
+    clocks.start()
+    for n_side in (a.calib_n, 64):
+        P = workloads.calibration_problem(n=n_side, n_steps=a.calib_steps)
+        s = P.scenario
+        K = P.n_steps
+        with calib.Calibration(s, K, P.gauges, device=dev) as cal:
+            _, gh, k_obs = cal.run(P.manning_true)
+            obs = np.zeros((K, len(P.gauges)))
+            obs[:k_obs] = gh
+            cal.set_observations(obs)
+            cols = np.arange(s.shape[1])
+            for _ in range(max(a.warmup, 3)):
+                cal.run(s.manning)
+            cal.tangent_lanes(s.manning, dn=np.ones((2,) + s.shape))
+            torch.cuda.synchronize(dev)
+
+            def timed(fn):
+                t0 = time.perf_counter()
+                out = fn()
+                torch.cuda.synchronize(dev)
+                return time.perf_counter() - t0, out
+
+            f_s, _ = timed(lambda: cal.run(s.manning))
+            g_s, (_, g) = timed(lambda: cal.gradient(s.manning))
+            rows = []
+            for Pn in counts:
+                zone = (cols * Pn) // s.shape[1]
+                dn = np.stack([np.broadcast_to((zone == p).astype(float), s.shape)
+                               for p in range(Pn)])
+                sc_s, sc = timed(lambda: [cal.tangent(s.manning, dn=dn[p])[1] for p in range(Pn)])
+                vm_s, (_, dJ) = timed(lambda: cal.tangent_lanes(s.manning, dn=dn))
+                same = bool(np.array_equal(np.array(sc), dJ))
+                zs = np.array([np.sum(g[:, zone == p]) for p in range(Pn)])
+                rel = float(np.max(np.abs(zs - dJ) / np.maximum(np.abs(dJ), 1e-300)))
+                rows.append({"P": Pn, "scalar_s": d.max(sc_s), "vector_s": d.max(vm_s),
+                             "scalar_vs_forward": d.max(sc_s) / d.max(f_s),
+                             "vector_vs_forward": d.max(vm_s) / d.max(f_s),
+                             "vector_per_param": (d.max(vm_s) / d.max(f_s)) / Pn,
+                             "lanes_equal_scalar_runs": same,
+                             "adjoint_zone_sums_max_rel": rel})
+                t_all += sc_s + vm_s
+        by_grid[f"{n_side}x{n_side}"] = {"cells": s.n_cells, "misfit_steps": K,
+                                         "forward_s": d.max(f_s), "gradient_s": d.max(g_s),
+                                         "gradient_vs_forward": d.max(g_s) / d.max(f_s),
+                                         "rows": rows}
+    clk = clocks.stop()
+    main_rows = by_grid[f"{a.calib_n}x{a.calib_n}"]["rows"]
+    p16 = [r for r in main_rows if r["P"] == 16][0]
+    line = {"metric": "16-parameter forward-mode gradient time / forward solve time (vector mode)",
+            "value": p16["vector_vs_forward"], "unit": "x", "n_gpus": d.world,
+            "steps": len(counts), "warmup": max(a.warmup, 3), "higher_is_better": False,
+            "scaling": "replicas", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded valley, log-normal Manning field, hidden-field gauges)",
+            "config": {"workload": f"zonal Manning derivatives (P vertical stripes) of a 16-gauge "
+                                   f"misfit over {a.calib_steps} steps, valley {a.calib_n}x"
+                                   f"{a.calib_n} and 64x64, dx 5 m",
+                       "parallelism": "replicas"},
+            "by_grid": by_grid,
+            "gpu_launches": int(a.calib_steps) * 5 * sum(counts) * 2, "clocks": clk}
+    if d.rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def run_serve(a, d: Dist):
     """An arrival stream through the continuous-batching server (hf_server_*)
     against a sequential plain solve per request (hf_sim run_until, FIFO, one
@@ -642,6 +730,8 @@ def main():
             run_adjoint(a, d)
         elif a.workload == "serve":
             run_serve(a, d)
+        elif a.workload == "lanes":
+            run_lanes(a, d)
         else:
             run_ours(a, d)
     finally:

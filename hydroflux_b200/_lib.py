@@ -72,6 +72,8 @@ PROTOTYPES = {
     "hf_calib_set_observations": (C.c_int, [_VP, _D]),
     "hf_calib_run": (C.c_int, [_VP, _D, C.c_int, _D, _D, C.POINTER(C.c_int64)]),
     "hf_tangent": (C.c_int, [_VP, _D, _D, _D, _D, _D, _D, _D]),
+    "hf_tangent_lanes": (C.c_int, [_VP, _D, C.c_int64, _D, _D, _D, _D, _D, _D]),
+    "hf_calib_lane_state": (C.c_int, [_VP, C.c_int64, _D, _D, _D]),
     "hf_grad_manning": (C.c_int, [_VP, _D, _D, _D, _D, _D, _D]),
     "hf_calib_final_state": (C.c_int, [_VP, _D, _D, _D, _D, _D, _D]),
     "hf_calib_dt": (C.c_int, [_VP, _D, C.POINTER(C.c_int64)]),

@@ -77,6 +77,31 @@ class Calibration:
         raise_for(lib().hf_tangent(self._h, *[_dp(a) for a in arrs], C.byref(J), C.byref(dJ)))
         return J.value, dJ.value
 
+    def tangent_lanes(self, manning, dn=None, dh0=None, dhu0=None, dhv0=None):
+        """Vector mode (DualN, autograd/src/dual_n.rs): (J, dJ[lanes]) for
+        `lanes` directions in one run. Each direction argument is None or an
+        array of shape (lanes, rows, cols); the lane count is their first
+        dimension. Every lane equals `tangent` along its direction bitwise."""
+        dirs = [a for a in (dn, dh0, dhu0, dhv0) if a is not None]
+        if not dirs:
+            raise ValueError("give at least one direction array of shape (lanes, rows, cols)")
+        lanes = int(np.shape(dirs[0])[0])
+        n = _f64(manning, self.ncell)
+        arrs = [None if a is None else _f64(a, lanes * self.ncell) for a in (dn, dh0, dhu0, dhv0)]
+        J = C.c_double()
+        dJ = np.zeros(lanes)
+        raise_for(lib().hf_tangent_lanes(self._h, _dp(n), lanes, *[_dp(a) for a in arrs],
+                                         C.byref(J), _dp(dJ)))
+        self._lanes = lanes
+        return J.value, dJ
+
+    def lane_state(self, lane: int) -> dict:
+        """Final tangent (dh, dhu, dhv) of one lane of the last tangent_lanes."""
+        out = {k: np.zeros(self.shape) for k in ("dh", "dhu", "dhv")}
+        raise_for(lib().hf_calib_lane_state(self._h, int(lane), *[_dp(out[k]) for k in
+                                                                  ("dh", "dhu", "dhv")]))
+        return out
+
     def gradient(self, manning, initial_state: bool = False):
         """(J, dJ/dn) or, with initial_state, (J, dJ/dn, (dJ/dh0, dJ/dhu0, dJ/dhv0))."""
         n = _f64(manning, self.ncell)

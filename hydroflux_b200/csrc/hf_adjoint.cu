@@ -693,13 +693,16 @@ __global__ void k_calib_pre(const Ctrl* c, double* dts, double* ts, long long ca
 
 __global__ void k_calib_post(const Ctrl* c, const double* __restrict__ h,
                              const double* __restrict__ dh, const int64_t* __restrict__ cells,
-                             int n_gauges, double* gauge_h, double* gauge_dh, long long cap) {
+                             int n_gauges, double* gauge_h, double* gauge_dh, long long cap,
+                             int lanes, long long lane_stride) {
   if (!c->active) return;
   const long long k = c->steps - 1;
   if (k < 0 || k >= cap) return;
   for (int g = threadIdx.x; g < n_gauges; g += blockDim.x) {
     gauge_h[k * n_gauges + g] = h[cells[g]];
-    if (dh) gauge_dh[k * n_gauges + g] = dh[cells[g]];
+    if (dh)
+      for (int l = 0; l < lanes; ++l)
+        gauge_dh[((long long)l * cap + k) * n_gauges + g] = dh[l * lane_stride + cells[g]];
   }
 }
 
@@ -771,10 +774,10 @@ int launch_calib_pre(const Ctrl* c, double* dts, double* ts, long long cap, void
 
 int launch_calib_post(const Ctrl* c, const double* h, const double* dh, const int64_t* cells,
                       int n_gauges, double* gauge_h, double* gauge_dh, long long cap,
-                      void* stream) {
+                      void* stream, int lanes, long long lane_stride) {
   if (n_gauges <= 0) return 0;
   k_calib_post<<<1, 128, 0, (cudaStream_t)stream>>>(c, h, dh, cells, n_gauges, gauge_h, gauge_dh,
-                                                    cap);
+                                                    cap, lanes, lane_stride);
   return cuda_rc(cudaGetLastError());
 }
 

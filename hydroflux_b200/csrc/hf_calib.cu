@@ -122,6 +122,13 @@ struct hf_calib {
   int64_t last_run = 0;  // steps of the last run without replay
   bool have_dts = false;
   std::vector<double> obs_host;
+  // vector-mode tangent (hf_tangent_lanes): lanes x cells per array
+  int lanes_cap = 0, last_lanes = 0;
+  double* dUL[3] = {nullptr, nullptr, nullptr};
+  double* dU1L[3] = {nullptr, nullptr, nullptr};
+  double* dnL = nullptr;
+  double* gdhL = nullptr;                      // [lane][K][G]
+  double* Ualt[3] = {nullptr, nullptr, nullptr};  // second value buffer (no in-place stage 2)
 };
 
 namespace {
@@ -461,8 +468,11 @@ void destroy_calib(hf_calib* c) {
     if (s) cudaStreamDestroy(s);
   for (int f = 0; f < 3; ++f)
     for (void* p : {(void*)c->U[f], (void*)c->U1[f], (void*)c->dU[f], (void*)c->dU1[f],
-                    (void*)c->lam[f], (void*)c->lam1[f], (void*)c->lamun[f]})
+                    (void*)c->lam[f], (void*)c->lam1[f], (void*)c->lamun[f], (void*)c->dUL[f],
+                    (void*)c->dU1L[f], (void*)c->Ualt[f]})
       ptrs.push_back(p);
+  ptrs.push_back(c->dnL);
+  ptrs.push_back(c->gdhL);
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (c->h_ctrl) cudaFreeHost(c->h_ctrl);
@@ -479,6 +489,96 @@ int upload_tangent_init(hf_calib* c, const double* dh0, const double* dhu0, cons
     else
       C_CUDA(cudaMemsetAsync(c->dU[f], 0, bytes, c->stream));
   }
+  return HF_OK;
+}
+
+void free_lanes(hf_calib* c) {
+  for (int f = 0; f < 3; ++f) {
+    for (double** p : {&c->dUL[f], &c->dU1L[f]})
+      if (*p) {
+        cudaFree(*p);
+        *p = nullptr;
+      }
+  }
+  for (double** p : {&c->dnL, &c->gdhL})
+    if (*p) {
+      cudaFree(*p);
+      *p = nullptr;
+    }
+  c->lanes_cap = 0;
+}
+
+int alloc_lanes(hf_calib* c, int lanes) {
+  if (c->lanes_cap >= lanes) return HF_OK;
+  C_CUDA(cudaStreamSynchronize(c->stream));
+  free_lanes(c);
+  const size_t n = (size_t)lanes * (size_t)c->ncell;
+  for (int f = 0; f < 3; ++f) {
+    C_TRY(calloc_dev(&c->dUL[f], n));
+    C_TRY(calloc_dev(&c->dU1L[f], n));
+    if (!c->Ualt[f]) C_TRY(calloc_dev(&c->Ualt[f], (size_t)c->ncell));
+  }
+  C_TRY(calloc_dev(&c->dnL, n));
+  C_TRY(calloc_dev(&c->gdhL, (size_t)lanes * (size_t)std::max<int64_t>(c->K * c->G, 1)));
+  c->lanes_cap = lanes;
+  return HF_OK;
+}
+
+// Vector-mode tangent run: the mode-2 run of forward_run with `lanes`
+// tangents at once (grid.y = lane). Lane 0 writes the values; stage 2
+// writes them into the other value buffer (no in-place combination, since
+// other lanes still read U^n), and the buffers swap after every step.
+int forward_run_lanes(hf_calib* c, int lanes, int64_t* n_run) {
+  const size_t bytes = (size_t)c->ncell * sizeof(double);
+  double* h0[3] = {c->h0, c->hu0, c->hv0};
+  for (int f = 0; f < 3; ++f)
+    C_CUDA(cudaMemcpyAsync(c->U[f], h0[f], bytes, cudaMemcpyDeviceToDevice, c->stream));
+  C_TRY(init_ctrl(c, false));
+  const ForcingDev fd = c->forcing.dev();
+  const bool ssp = c->cfg.integrator == HF_SSPRK2;
+  const long long stride = (long long)c->ncell;
+  const int cap = stage_dual_grid_size(1 << 30, c->device);
+  const int grid = std::max(1, std::min(c->ntiles, (cap + lanes - 1) / lanes));
+  double* cur[3] = {c->U[0], c->U[1], c->U[2]};
+  double* nxt[3] = {c->Ualt[0], c->Ualt[1], c->Ualt[2]};
+  {
+    StageArgs a0 = calib_args(c, cur, c->U1, nullptr, 0, 0, c->ctrl, fd);
+    C_TRY(launch_cfl(a0, 1, c->grid, c->stream));
+  }
+  for (int64_t k = 0; k < c->K; ++k) {
+    StageArgs a1 = calib_args(c, cur, c->U1, nullptr, 0, 0, c->ctrl, fd);
+    StageArgs a2 = calib_args(c, c->U1, nxt, cur, ssp ? 1 : 0, 1, c->ctrl, fd);
+    with_tangent(a1, c, c->dUL, c->dU1L, nullptr);
+    with_tangent(a2, c, c->dU1L, c->dUL, c->dUL);
+    a1.tan.n = a2.tan.n = c->dnL;
+    a1.tan.lane_stride = a2.tan.lane_stride = stride;
+    C_TRY(launch_control(c->ctrl, c->dx, c->dy, fd, c->stream));
+    C_TRY(launch_calib_pre(c->ctrl, c->dts, c->ts, (long long)c->K, c->stream));
+    C_TRY(launch_stage_dual(a1, grid, c->stream, lanes));
+    if (ssp)
+      C_TRY(launch_stage_dual(a2, grid, c->stream, lanes));
+    else
+      C_TRY(launch_finalize_dual(a2, grid, c->stream, lanes));
+    C_TRY(launch_calib_post(c->ctrl, nxt[0], c->dUL[0], c->cells, (int)c->G, c->gh, c->gdhL,
+                            (long long)c->K, c->stream, lanes, stride));
+    // A step that did not run (the run had ended) leaves nxt unwritten.
+    for (int f = 0; f < 3; ++f) std::swap(cur[f], nxt[f]);
+    if ((k + 1) % 64 == 0 && k + 1 < c->K) {
+      C_CUDA(cudaMemcpyAsync(c->h_ctrl, c->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost,
+                             c->stream));
+      C_CUDA(cudaStreamSynchronize(c->stream));
+      if (!c->h_ctrl->active || c->h_ctrl->status != 0) break;
+    }
+  }
+  int64_t run = 0;
+  C_TRY(status_of_run(c, &run));
+  c->last_run = run;
+  c->have_dts = true;
+  // The values after the last step taken: step j wrote buffer (j odd ? Ualt : U).
+  if (run % 2 == 1)
+    for (int f = 0; f < 3; ++f)
+      C_CUDA(cudaMemcpyAsync(c->U[f], c->Ualt[f], bytes, cudaMemcpyDeviceToDevice, c->stream));
+  if (n_run) *n_run = run;
   return HF_OK;
 }
 
@@ -617,6 +717,73 @@ int hf_tangent(hf_calib* c, const double* manning, const double* dn, const doubl
   int64_t run = 0;
   C_TRY(forward_run(c, 2, false, &run));
   return misfit(c, run, true, J, dJ, nullptr);
+}
+
+int hf_tangent_lanes(hf_calib* c, const double* manning, int64_t n_lanes, const double* dn,
+                     const double* dh0, const double* dhu0, const double* dhv0, double* J,
+                     double* dJ) {
+  if (!c) return cfail(HF_ERR_INVALID_ARG, "null problem");
+  if (n_lanes < 1 || n_lanes > 1024)
+    return cfail(HF_ERR_INVALID_ARG, "n_lanes must be in 1..1024");
+  Guard g(c->device);
+  C_TRY(upload_manning(c, manning));
+  const int L = (int)n_lanes;
+  C_TRY(alloc_lanes(c, L));
+  const size_t n = (size_t)L * (size_t)c->ncell, bytes = n * sizeof(double);
+  if (dn)
+    C_CUDA(cudaMemcpyAsync(c->dnL, dn, bytes, cudaMemcpyHostToDevice, c->stream));
+  else
+    C_CUDA(cudaMemsetAsync(c->dnL, 0, bytes, c->stream));
+  const double* src[3] = {dh0, dhu0, dhv0};
+  for (int f = 0; f < 3; ++f) {
+    if (src[f])
+      C_CUDA(cudaMemcpyAsync(c->dUL[f], src[f], bytes, cudaMemcpyHostToDevice, c->stream));
+    else
+      C_CUDA(cudaMemsetAsync(c->dUL[f], 0, bytes, c->stream));
+  }
+  int64_t run = 0;
+  C_TRY(forward_run_lanes(c, L, &run));
+  c->last_lanes = L;
+  // J from the gauge values, dJ per lane from that lane's gauge tangents,
+  // in the same step-major, gauge-minor order as hf_tangent.
+  const size_t m = (size_t)(run * c->G);
+  std::vector<double> gh(m ? m : 1), gdh(m ? m * (size_t)L : 1);
+  if (m) {
+    C_CUDA(cudaMemcpyAsync(gh.data(), c->gh, m * sizeof(double), cudaMemcpyDeviceToHost,
+                           c->stream));
+    for (int l = 0; l < L; ++l)
+      C_CUDA(cudaMemcpyAsync(gdh.data() + (size_t)l * m, c->gdhL + (size_t)l * c->K * c->G,
+                             m * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    C_CUDA(cudaStreamSynchronize(c->stream));
+  }
+  double j = 0.0;
+  for (size_t i = 0; i < m; ++i) {
+    const double r = gh[i] - c->obs_host[i];
+    j += r * r;
+  }
+  if (J) *J = j;
+  if (dJ)
+    for (int l = 0; l < L; ++l) {
+      double dj = 0.0;
+      for (size_t i = 0; i < m; ++i) dj += 2.0 * (gh[i] - c->obs_host[i]) * gdh[(size_t)l * m + i];
+      dJ[l] = dj;
+    }
+  return HF_OK;
+}
+
+int hf_calib_lane_state(hf_calib* c, int64_t lane, double* dh, double* dhu, double* dhv) {
+  if (!c) return cfail(HF_ERR_INVALID_ARG, "null problem");
+  if (lane < 0 || lane >= c->last_lanes)
+    return cfail(HF_ERR_INVALID_ARG, "no such lane in the last hf_tangent_lanes run");
+  Guard g(c->device);
+  C_CUDA(cudaStreamSynchronize(c->stream));
+  const size_t bytes = (size_t)c->ncell * sizeof(double);
+  double* outs[3] = {dh, dhu, dhv};
+  for (int f = 0; f < 3; ++f)
+    if (outs[f])
+      C_CUDA(cudaMemcpy(outs[f], c->dUL[f] + (size_t)lane * c->ncell, bytes,
+                        cudaMemcpyDeviceToHost));
+  return HF_OK;
 }
 
 int hf_grad_manning(hf_calib* c, const double* manning, double* J, double* grad_n,

@@ -129,6 +129,9 @@ struct TanPtrs {
   const double* un_hu = nullptr;
   const double* un_hv = nullptr;
   const double* n = nullptr;  // Manning tangent
+  // Vector mode: blockIdx.y is the tangent lane; lane l's tangent arrays
+  // start lane_stride doubles after lane l-1's (0: one lane).
+  long long lane_stride = 0;
 };
 
 struct StageArgs {
@@ -186,8 +189,11 @@ int stage_grid_size(int tiles, int device);
 size_t stage_smem_bytes();
 // DualD tangent stage / finalize (same arguments; tangent arrays in a.tan).
 int stage_dual_grid_size(int tiles, int device);
-int launch_stage_dual(const StageArgs& a, int grid, void* stream);
-int launch_finalize_dual(const StageArgs& a, int grid, void* stream);
+// lanes > 1 (vector mode): one grid of `grid` CTAs per tangent lane
+// (blockIdx.y), a.tan.lane_stride apart; lane 0 alone writes the values, so
+// a.out_* must not alias a.in_* or a.un_* then.
+int launch_stage_dual(const StageArgs& a, int grid, void* stream, int lanes = 1);
+int launch_finalize_dual(const StageArgs& a, int grid, void* stream, int lanes = 1);
 
 // Adjoint of one stage (hf_adjoint.cu). `a` is the stage's forward arguments
 // (with combine / finalize as run); lam_* the adjoint of its output. Writes
@@ -208,9 +214,10 @@ int launch_adj_gather(int nr, int nc, int tiles_x, int tiles_y, const double* ha
 int launch_adj_seed(double* lam_h, const int64_t* cells, int n_gauges, const double* gauge_h,
                     const double* obs, void* stream);
 int launch_calib_pre(const Ctrl* c, double* dts, double* ts, long long cap, void* stream);
+// gauge_dh of lane l at [l][cap][n_gauges], read from dh + l * lane_stride.
 int launch_calib_post(const Ctrl* c, const double* h, const double* dh, const int64_t* cells,
                       int n_gauges, double* gauge_h, double* gauge_dh, long long cap,
-                      void* stream);
+                      void* stream, int lanes = 1, long long lane_stride = 0);
 int launch_calib_rewind(Ctrl* c, const double* ts, long long k, void* stream);
 
 // Sets the calling thread's hf_last_error() message and returns `code`.

@@ -15,6 +15,8 @@
 // point operation rounds like the reference's Rust f64 code.
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include <cstdio>
 
 #include "hf_device.cuh"
@@ -28,7 +30,30 @@ namespace hf {
 template <class T> struct StageOcc { static constexpr int value = HF_MIN_BLOCKS; };
 template <> struct StageOcc<DualD> { static constexpr int value = 1; };
 
-// One stage of one grid over a persistent tile loop.
+// The arguments of tangent lane `lane`: its tangent arrays, and no value
+// outputs unless it is lane 0 (the values are the same in every lane).
+__device__ void lane_args(const StageArgs& A, int lane, StageArgs& L) {
+  L = A;
+  if (lane == 0) return;
+  const long long o = (long long)lane * A.tan.lane_stride;
+  auto shift = [o](const double* p) { return p ? p + o : p; };
+  auto shift_w = [o](double* p) { return p ? p + o : p; };
+  L.tan.in_h = shift(A.tan.in_h);
+  L.tan.in_hu = shift(A.tan.in_hu);
+  L.tan.in_hv = shift(A.tan.in_hv);
+  L.tan.out_h = shift_w(A.tan.out_h);
+  L.tan.out_hu = shift_w(A.tan.out_hu);
+  L.tan.out_hv = shift_w(A.tan.out_hv);
+  L.tan.un_h = shift(A.tan.un_h);
+  L.tan.un_hu = shift(A.tan.un_hu);
+  L.tan.un_hv = shift(A.tan.un_hv);
+  L.tan.n = shift(A.tan.n);
+  L.out_h = L.out_hu = L.out_hv = nullptr;
+}
+
+// One stage of one grid over a persistent tile loop. For T = DualD,
+// blockIdx.y is the tangent lane (vector mode); the CFL reduction and the
+// clock belong to lane 0.
 template <class T>
 __global__ void __launch_bounds__(NTHREADS, StageOcc<T>::value) k_stage(const StageArgs A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -37,9 +62,18 @@ __global__ void __launch_bounds__(NTHREADS, StageOcc<T>::value) k_stage(const St
   const int ntiles = A.tiles_x * A.tiles_y;
   double sxm = 0.0, sym = 0.0;
   unsigned long long nonfin = 0;
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
-    stage_tile<T>(A, S, tile, sxm, sym, nonfin);
-  if (A.finalize) {
+  if constexpr (std::is_same<T, DualD>::value) {
+    __shared__ __align__(16) unsigned char lane_raw[sizeof(StageArgs)];
+    StageArgs& L = *reinterpret_cast<StageArgs*>(lane_raw);
+    if (threadIdx.x == 0) lane_args(A, blockIdx.y, L);
+    __syncthreads();
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
+      stage_tile<T>(L, S, tile, sxm, sym, nonfin);
+  } else {
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
+      stage_tile<T>(A, S, tile, sxm, sym, nonfin);
+  }
+  if (A.finalize && blockIdx.y == 0) {
     block_reduce_speeds(sxm, sym, nonfin, A.ctrl);
     if (blockIdx.x == 0 && threadIdx.x == 0) commit_clock(A.ctrl);
   }
@@ -93,14 +127,13 @@ __global__ void __launch_bounds__(NTHREADS, HF_MIN_BLOCKS)
 
 // Epilogue of a forward-Euler step: friction, forcings and the CFL
 // reduction of the stage result (in_*) into the state (out_*).
+// The forward-Euler finalize of one grid over its tiles (friction, forcings,
+// CFL contributions); returns the CTA's speed maxima.
 template <class T>
-__global__ void __launch_bounds__(NTHREADS) k_finalize(const StageArgs A) {
-  Ctrl* ctrl = A.ctrl;
-  if (!ctrl->active) return;
+__device__ void finalize_tiles(const StageArgs& A, Ctrl* ctrl, double& sxm, double& sym,
+                               unsigned long long& nonfin) {
   const double dt = ctrl->dt;
   const int ntiles = A.tiles_x * A.tiles_y;
-  double sxm = 0.0, sym = 0.0;
-  unsigned long long nonfin = 0;
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int tyi = tile / A.tiles_x;
     const int gi0 = tyi * TY, gj0 = (tile - tyi * A.tiles_x) * TX;
@@ -124,6 +157,26 @@ __global__ void __launch_bounds__(NTHREADS) k_finalize(const StageArgs A) {
       Field<T>::st(A.out_hv, A.tan.out_hv, g, hv);
     }
   }
+}
+
+// Forward-Euler finalize kernel. For T = DualD, blockIdx.y is the tangent
+// lane, as in k_stage.
+template <class T>
+__global__ void __launch_bounds__(NTHREADS) k_finalize(const StageArgs A) {
+  Ctrl* ctrl = A.ctrl;
+  if (!ctrl->active) return;
+  double sxm = 0.0, sym = 0.0;
+  unsigned long long nonfin = 0;
+  if constexpr (std::is_same<T, DualD>::value) {
+    __shared__ __align__(16) unsigned char lane_raw[sizeof(StageArgs)];
+    StageArgs& L = *reinterpret_cast<StageArgs*>(lane_raw);
+    if (threadIdx.x == 0) lane_args(A, blockIdx.y, L);
+    __syncthreads();
+    finalize_tiles<T>(L, ctrl, sxm, sym, nonfin);
+  } else {
+    finalize_tiles<T>(A, ctrl, sxm, sym, nonfin);
+  }
+  if (blockIdx.y != 0) return;  // the CFL reduction and the clock belong to lane 0
   block_reduce_speeds(sxm, sym, nonfin, ctrl);
   if (blockIdx.x == 0 && threadIdx.x == 0) commit_clock(ctrl);
 }
@@ -482,13 +535,14 @@ int launch_finalize(const StageArgs& a, int grid, void* stream) {
 
 // DualD (tangent) stage and finalize: value arrays in a.in_* / a.out_* /
 // a.un_* / a.n, tangent arrays in a.tan. Grid from stage_dual_grid_size().
-int launch_stage_dual(const StageArgs& a, int grid, void* stream) {
-  k_stage<DualD><<<grid, NTHREADS, sizeof(StageSmemT<DualD>), (cudaStream_t)stream>>>(a);
+int launch_stage_dual(const StageArgs& a, int grid, void* stream, int lanes) {
+  k_stage<DualD><<<dim3(grid, lanes), NTHREADS, sizeof(StageSmemT<DualD>),
+                   (cudaStream_t)stream>>>(a);
   return cuda_rc(cudaGetLastError());
 }
 
-int launch_finalize_dual(const StageArgs& a, int grid, void* stream) {
-  k_finalize<DualD><<<grid, NTHREADS, 0, (cudaStream_t)stream>>>(a);
+int launch_finalize_dual(const StageArgs& a, int grid, void* stream, int lanes) {
+  k_finalize<DualD><<<dim3(grid, lanes), NTHREADS, 0, (cudaStream_t)stream>>>(a);
   return cuda_rc(cudaGetLastError());
 }
 

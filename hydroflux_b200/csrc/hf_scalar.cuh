@@ -104,8 +104,10 @@ template <> struct Field<DualD> {
   __device__ static DualD ld(const double* v, const double* d, int64_t g) {
     return DualD{v[g], d ? d[g] : 0.0};
   }
+  // v == nullptr: a tangent lane other than the first, which leaves the
+  // (shared) value arrays to lane 0.
   __device__ static void st(double* v, double* d, int64_t g, DualD x) {
-    v[g] = x.v;
+    if (v) v[g] = x.v;
     d[g] = x.d;
   }
 };

@@ -305,6 +305,19 @@ int hf_calib_run(hf_calib* calib, const double* manning, int replay_dt, double* 
  * be NULL (zero). Returns J and its directional derivative dJ. */
 int hf_tangent(hf_calib* calib, const double* manning, const double* dn, const double* dh0,
                const double* dhu0, const double* dhv0, double* J, double* dJ);
+/* Vector mode (DualN<N>, autograd/src/dual_n.rs; used by
+ * solver-2d/examples/m1_forward_scaling.rs): n_lanes directions in one run.
+ * dn, dh0, dhu0 and dhv0 hold n_lanes consecutive arrays of one value per
+ * cell (any may be NULL: zero); dJ receives n_lanes values. Each lane is
+ * bit-identical to hf_tangent along that direction. The lanes run side by
+ * side in one launch per stage (a grid per lane), so on grids too small to
+ * fill the GPU the extra lanes cost little. 1 <= n_lanes <= 1024. */
+int hf_tangent_lanes(hf_calib* calib, const double* manning, int64_t n_lanes, const double* dn,
+                     const double* dh0, const double* dhu0, const double* dhv0, double* J,
+                     double* dJ);
+/* Final tangent of one lane of the last hf_tangent_lanes run (any pointer
+ * may be NULL). */
+int hf_calib_lane_state(hf_calib* calib, int64_t lane, double* dh, double* dhu, double* dhv);
 /* Reverse mode: J and dJ/dn (one value per cell); the gradient with respect
  * to the initial state is written when grad_h0 / grad_hu0 / grad_hv0 are
  * non-NULL. */

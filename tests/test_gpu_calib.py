@@ -208,3 +208,57 @@ def test_gradient_against_central_differences(gpu):
             Jm, _, _ = cal.run(n - eps * n * v, replay_dt=True)
             fd = (Jp - Jm) / (2 * eps)
             assert abs(fd - ad) <= 2e-5 * abs(ad), (k, fd, ad)
+
+
+@pytest.mark.parametrize("name", PROBLEMS)
+def test_tangent_lanes_equal_single_tangents(gpu, name):
+    """Vector mode (DualN, autograd/src/dual_n.rs): every lane of one
+    hf_tangent_lanes run equals hf_tangent along that direction bit for bit
+    (dJ and the final tangent state), and the values equal a plain run."""
+    calib, workloads = gpu
+    s, K, gauges = problem(workloads, name)
+    lanes = 5
+    with calib.Calibration(s, K, gauges) as cal:
+        observations(cal, s, K, len(gauges), 7)
+        J0, _, _ = cal.run(s.manning)
+        ref_state = cal.final_state()
+        rng = np.random.default_rng(8)
+        ds = [directions(rng, s) for _ in range(lanes)]
+        stack = {k: np.stack([d[k] for d in ds]) for k in ds[0]}
+        J, dJ = cal.tangent_lanes(s.manning, **stack)
+        st = cal.final_state()
+        lane_states = [cal.lane_state(l) for l in range(lanes)]
+        assert J == J0
+        for k in ("h", "hu", "hv"):
+            assert np.array_equal(st[k], ref_state[k]), k
+        for l, d in enumerate(ds):
+            J1, dJ1 = cal.tangent(s.manning, **d)
+            one = cal.final_state()
+            assert J1 == J and dJ1 == dJ[l], (l, dJ1, dJ[l])
+            for k in ("dh", "dhu", "dhv"):
+                assert np.array_equal(lane_states[l][k], one[k]), (l, k)
+
+
+def test_tangent_lanes_zonal_gradient(gpu):
+    """The forward-scaling use (solver-2d/examples/m1_forward_scaling.rs):
+    P zonal Manning parameters in vertical stripes, all P derivatives in one
+    vector-mode run; they equal the adjoint gradient summed over each zone."""
+    calib, workloads = gpu
+    s, K, gauges = problem(workloads, "valley")
+    P = 8
+    cols = np.arange(s.shape[1])
+    zone = (cols * P) // s.shape[1]
+    dn = np.stack([np.broadcast_to((zone == p).astype(float), s.shape) for p in range(P)])
+    with calib.Calibration(s, K, gauges) as cal:
+        observations(cal, s, K, len(gauges), 9)
+        J, dJ = cal.tangent_lanes(s.manning, dn=dn)
+        Jg, g = cal.gradient(s.manning)
+        assert J == Jg
+        for p in range(P):
+            want = np.sum(g[:, zone == p])
+            scale = np.sum(np.abs(g[:, zone == p]))
+            assert abs(dJ[p] - want) <= 1e-9 * max(scale, abs(want)), (p, dJ[p], want)
+        with pytest.raises(ValueError):
+            cal.tangent_lanes(s.manning, dn=np.zeros((1025,) + s.shape))
+        with pytest.raises(ValueError):
+            cal.lane_state(P)
