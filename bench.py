@@ -574,6 +574,7 @@ def run_lanes(a, d: Dist):
             for _ in range(max(a.warmup, 3)):
                 cal.run(s.manning)
             cal.tangent_lanes(s.manning, dn=np.ones((2,) + s.shape))
+            cal.gradient(s.manning)  # allocates the adjoint's buffers
             torch.cuda.synchronize(dev)
 
             def timed(fn):

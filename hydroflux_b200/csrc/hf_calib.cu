@@ -537,8 +537,10 @@ int forward_run_lanes(hf_calib* c, int lanes, int64_t* n_run) {
   const ForcingDev fd = c->forcing.dev();
   const bool ssp = c->cfg.integrator == HF_SSPRK2;
   const long long stride = (long long)c->ncell;
+  // One wave: lanes x grid CTAs within the resident capacity (a second,
+  // partial wave would double the stage time).
   const int cap = stage_dual_grid_size(1 << 30, c->device);
-  const int grid = std::max(1, std::min(c->ntiles, (cap + lanes - 1) / lanes));
+  const int grid = std::max(1, std::min(c->ntiles, cap / lanes));
   double* cur[3] = {c->U[0], c->U[1], c->U[2]};
   double* nxt[3] = {c->Ualt[0], c->Ualt[1], c->Ualt[2]};
   {
