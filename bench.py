@@ -140,16 +140,36 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """DRAM bytes per stage launch per cell from the committed ncu summary."""
+def profiled_figure(key):
+    """A per-cell figure of the stage kernel from the committed ncu summary."""
     path = os.path.join(ROOT, "profiles", "stage_kernel_traffic.txt")
     try:
         for line in open(path):
-            if line.startswith("dram_bytes_per_cell_per_launch:"):
+            if line.startswith(key + ":"):
                 return float(line.split(":")[1])
     except OSError:
         pass
     return None
+
+
+def profiled_traffic():
+    """DRAM bytes per stage launch per cell from the committed ncu summary."""
+    return profiled_figure("dram_bytes_per_cell_per_launch")
+
+
+def issue_roof(value, clk):
+    """The bound the stage kernel actually runs against: instruction issue.
+    Warp instructions per cell-update from the committed ncu summary; the
+    peak issues one warp instruction per scheduler per cycle (4 per SM) on
+    every SM at the SM clock measured during the timed region."""
+    per_cell = profiled_figure("warp_instructions_per_cell_update")
+    if per_cell is None or not clk or not clk.get("sm_mhz"):
+        return None
+    import torch
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    peak = sms * 4 * clk["sm_mhz"] * 1e6 / per_cell
+    return {"unit": UNIT, "achieved": value, "peak": peak, "frac": value / peak,
+            "warp_instructions_per_cell_update": per_cell, "sms": sms, "sm_mhz": clk["sm_mhz"]}
 
 
 # ---------------------------------------------------------------- workload
@@ -296,7 +316,8 @@ def run_ours(a, d: Dist):
                      "frac": achieved_gbs / peak, "peak_source": peak_kind,
                      "traffic": (traffic_per_cell * cells) if traffic_per_cell else None,
                      "kernel": "k_stage_pf", "alg_bytes_per_launch": bytes_per_launch,
-                     "avg_launch_ms": avg_stage_s * 1e3, "launches": stage_launches},
+                     "avg_launch_ms": avg_stage_s * 1e3, "launches": stage_launches,
+                     "issue": issue_roof(value / d.world, clk)},
         "cpu_baseline": cpu,
         "clocks": clk,
     }
