@@ -89,6 +89,18 @@ double series_eval_u(const double* ts, const double* vs, int64_t n, double t, co
   return series_eval(ts, vs, n, t / u.t_div) * u.v_mul / u.v_div;
 }
 
+// Control-point recorder of hfo_sim_run (hf_sim_set_gauges): after every
+// step, peak = fold(0.0, f64::max) and last = h at each gauge cell
+// (uk_ea_test8a_official.rs:219-246). Set by hfo_set_gauges, the buffers
+// are the caller's; n = 0 disables it.
+struct GaugeRec {
+  int64_t n = 0;
+  const int64_t* cells = nullptr;
+  double* peak = nullptr;
+  double* last = nullptr;
+};
+GaugeRec g_gauges;
+
 // Forcing descriptor (see hf_sim_set_rain / hf_sim_set_point_sources).
 struct Forcing {
   int64_t n_rain = 0;
@@ -328,6 +340,11 @@ int hfo_sim_run(int64_t nr, int64_t nc, double dx, double dy, const double* z, c
   Forcing f{n_rain, rain_t, rain_v, n_src, rows, cols, offs, src_t, src_q};
   uint64_t budget = cfg->max_steps;
   int64_t taken = 0;
+  const GaugeRec gr = g_gauges;
+  for (int64_t k = 0; k < gr.n; ++k) {
+    gr.peak[k] = std::fmax(0.0, s[gr.cells[k]].h);
+    gr.last[k] = s[gr.cells[k]].h;
+  }
   rc = HF_OK;
   while (*t_io < t_target) {
     if (stop_after >= 0 && taken >= stop_after) break;
@@ -345,11 +362,20 @@ int hfo_sim_run(int64_t nr, int64_t nc, double dx, double dy, const double* z, c
       break;
     }
     if (dt_log && taken < dt_log_cap) dt_log[taken] = dt;
+    for (int64_t k = 0; k < gr.n; ++k) {
+      const double v = s[gr.cells[k]].h;
+      gr.peak[k] = std::fmax(gr.peak[k], v);
+      gr.last[k] = v;
+    }
     ++taken;
     --budget;
   }
   store(s, h, hu, hv);
   return rc;
+}
+
+void hfo_set_gauges(int64_t n, const int64_t* cells, double* peak, double* last) {
+  g_gauges = GaugeRec{n, cells, peak, last};
 }
 
 // One Simulation::step(dt_cap) (+ forcings); t/steps in-out.

@@ -40,6 +40,8 @@ def lib():
         _LIB.hfo_pow_cr.argtypes = [C.c_double, C.c_int]
         _LIB.hfo_set_series_units.restype = None
         _LIB.hfo_set_series_units.argtypes = [C.c_double] * 6
+        _LIB.hfo_set_gauges.restype = None
+        _LIB.hfo_set_gauges.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]
     return _LIB
 
 
@@ -215,9 +217,11 @@ class Forcing:
 
 
 def sim_run(z, n, dx, dy, h, hu, hv, cfg, t_target, forcing=None, stop_after=-1, t0=0.0,
-            steps0=0, dt_log_cap=0):
+            steps0=0, dt_log_cap=0, gauges=None):
     """Simulation::run_until semantics (+ forcings). Returns dict with state,
-    t, steps, status, dts (first dt_log_cap step sizes) and err_dt."""
+    t, steps, status, dts (first dt_log_cap step sizes) and err_dt; with
+    gauges (flat cell indices), also their peaks (fold(0.0, max) over the
+    initial and every stepped depth) and last depths."""
     z = _f64(z)
     n = _f64(n) if n is not None else np.zeros_like(z)
     h, hu, hv = _f64(h).copy(), _f64(hu).copy(), _f64(hv).copy()
@@ -226,14 +230,30 @@ def sim_run(z, n, dx, dy, h, hu, hv, cfg, t_target, forcing=None, stop_after=-1,
     steps = C.c_uint64(steps0)
     dts = np.zeros(max(dt_log_cap, 1))
     err_dt = C.c_double(0.0)
-    rc = lib().hfo_sim_run(C.c_int64(z.shape[0]), C.c_int64(z.shape[1]), C.c_double(dx),
+    g_cells = np.ascontiguousarray(gauges if gauges is not None else [], dtype=np.int64)
+    g_peak, g_last = np.zeros(max(len(g_cells), 1)), np.zeros(max(len(g_cells), 1))
+    lib().hfo_set_gauges(len(g_cells), g_cells.ctypes.data, g_peak.ctypes.data,
+                         g_last.ctypes.data)
+    try:
+        rc = _sim_run_call(z, n, dx, dy, h, hu, hv, cfg, t_target, forcing, stop_after, t, steps,
+                           dts, dt_log_cap, err_dt)
+    finally:
+        lib().hfo_set_gauges(0, None, None, None)
+    msg = lib().hfo_last_error().decode() if rc else ""
+    out = dict(h=h, hu=hu, hv=hv, t=t.value, steps=steps.value, status=rc, message=msg,
+               dts=dts[:min(dt_log_cap, steps.value - steps0)], err_dt=err_dt.value)
+    if gauges is not None:
+        out["gauge_peak"], out["gauge_last"] = g_peak[:len(g_cells)], g_last[:len(g_cells)]
+    return out
+
+
+def _sim_run_call(z, n, dx, dy, h, hu, hv, cfg, t_target, forcing, stop_after, t, steps, dts,
+                  dt_log_cap, err_dt):
+    return lib().hfo_sim_run(C.c_int64(z.shape[0]), C.c_int64(z.shape[1]), C.c_double(dx),
                            C.c_double(dy), _p(z), _p(n), _p(h), _p(hu), _p(hv), C.byref(cfg),
                            *forcing.args(), C.c_double(t_target), C.c_int64(stop_after),
                            C.byref(t), C.byref(steps), _p(dts), C.c_int64(dt_log_cap),
                            C.byref(err_dt))
-    msg = lib().hfo_last_error().decode() if rc else ""
-    return dict(h=h, hu=hu, hv=hv, t=t.value, steps=steps.value, status=rc, message=msg,
-                dts=dts[:min(dt_log_cap, steps.value - steps0)], err_dt=err_dt.value)
 
 
 def sim_step(z, n, dx, dy, h, hu, hv, cfg, dt_cap, forcing=None, t0=0.0, steps0=0):

@@ -168,3 +168,28 @@ def test_reference_decks(L, deck):
             ref = L.read_reference_stage(os.path.join(UK_EA, "test4/reference", f))
             assert ref.points == c.points and len(ref.times) > 100
     assert c.sim_time == 18000.0
+
+
+def test_oracle_gauge_recorder(L, oracle):
+    """The oracle's run records the same peaks and last depths as stepping
+    it one step at a time (the check the GPU gauges are held to)."""
+    from hydroflux_b200 import abi
+    O = oracle
+    rng = np.random.default_rng(13)
+    nr, nc = 9, 11
+    z = rng.uniform(0.0, 0.5, (nr, nc))
+    n = np.full((nr, nc), 0.03)
+    h0 = rng.uniform(0.0, 0.4, (nr, nc)) * (rng.uniform(size=(nr, nc)) > 0.3)
+    zero = np.zeros((nr, nc))
+    cfg = abi.make_config(max_dt=0.5)
+    cells = [0, 5 * nc + 3, nr * nc - 1, 5 * nc + 3]
+    r = O.sim_run(z, n, 1.0, 1.0, h0, zero, zero, cfg, 1e9, stop_after=40, gauges=cells)
+    h, hu, hv, t = h0, zero, zero, 0.0
+    peak = np.maximum(h0.ravel()[cells], 0.0)
+    for k in range(40):
+        s = O.sim_step(z, n, 1.0, 1.0, h, hu, hv, cfg, 1e9 - t, t0=t, steps0=k)
+        h, hu, hv, t = s["h"], s["hu"], s["hv"], s["t"]
+        peak = np.maximum(peak, h.ravel()[cells])
+    assert np.array_equal(r["gauge_peak"], peak)
+    assert np.array_equal(r["gauge_last"], h.ravel()[cells])
+    assert np.array_equal(r["h"], h)
