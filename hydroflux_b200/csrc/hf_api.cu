@@ -899,6 +899,9 @@ namespace {
 int check_grid(const hf_grid* g, hf_workspace* w) {
   if (!g) return fail(HF_ERR_INVALID_ARG, "null grid");
   HF_TRY(check_shape(g->n_rows, g->n_cols));
+  // Mesh2D's own checks (geometry.rs:59, 93: dx, dy strictly positive).
+  if (!(g->dx > 0.0) || !(g->dy > 0.0))
+    return fail(HF_ERR_INVALID_ARG, "dx and dy must be strictly positive");
   if (w && (w->nr != g->n_rows || w->nc != g->n_cols)) {
     char buf[128];
     std::snprintf(buf, sizeof buf, "workspace shape (%lld, %lld) must match mesh (%lld, %lld)",

@@ -8,8 +8,12 @@
 // sign(a) xor sign(b), and sqrt(+-0) is +-0. These helpers return that value
 // directly and otherwise compute the correctly rounded a / b or sqrt(x), so
 // they are bit-identical to `/` and `sqrt` for every input. The division
-// itself never sees the zero numerator (it divides 1 / b on those lanes and
-// discards the quotient), so predicated code avoids the slow path too.
+// itself never sees the zero numerator: it divides 1 / b on those lanes and
+// discards the quotient, so predicated code avoids the slow path too. The
+// substituted operand goes through an empty asm statement; without it the
+// compiler may fold it back into `a` (the quotient is unused on exactly the
+// lanes where they differ) and divide the zero after all, which measured
+// 96 instead of 28 instructions per division.
 #pragma once
 
 #include <cmath>
@@ -29,12 +33,26 @@ HF_ARITH_HD double div_rn(double a, double b) {
   const bool a_zero = (ia << 1) == 0;
   const bool b_regular = ((ib >> 52) & 0x7ff) != 0x7ff && (ib << 1) != 0;
   const bool shortcut = a_zero && b_regular;
-  const double q = (shortcut ? 1.0 : a) / b;
+  double num = shortcut ? 1.0 : a;
+  asm volatile("" : "+d"(num));
+  const double q = num / b;
   return shortcut ? __longlong_as_double((ia ^ ib) & (long long)0x8000000000000000ull) : q;
+}
+// a / b for a divisor known to be > 0 (compared greater than a positive
+// threshold, or a positive grid spacing; +inf allowed): then a zero
+// numerator's quotient is a itself, and the divisor needs no test.
+HF_ARITH_HD double div_rn_pos(double a, double b) {
+  const bool a_zero = (__double_as_longlong(a) << 1) == 0;
+  double num = a_zero ? 1.0 : a;
+  asm volatile("" : "+d"(num));
+  const double q = num / b;
+  return a_zero ? a : q;
 }
 HF_ARITH_HD double sqrt_rn(double x) {
   const bool zero = (__double_as_longlong(x) << 1) == 0;
-  const double s = sqrt(zero ? 1.0 : x);
+  double y = zero ? 1.0 : x;
+  asm volatile("" : "+d"(y));
+  const double s = sqrt(y);
   return zero ? x : s;
 }
 // +-0 and finiteness from the bit pattern (integer pipe, not the FP64 pipe).
@@ -44,6 +62,7 @@ HF_ARITH_HD bool is_finite(double x) {
 }
 #else
 HF_ARITH_HD double div_rn(double a, double b) { return a / b; }
+HF_ARITH_HD double div_rn_pos(double a, double b) { return a / b; }
 HF_ARITH_HD double sqrt_rn(double x) { return std::sqrt(x); }
 HF_ARITH_HD bool is_zero(double x) { return x == 0.0; }
 HF_ARITH_HD bool is_finite(double x) { return std::isfinite(x); }

@@ -92,8 +92,8 @@ __device__ __forceinline__ void hllc_normal(T h_l, T qn_l, T qt_l, T h_r, T qn_r
   }
   const T cl = wl ? r_sqrt_pos(h_l * GRAVITY) : Z;
   const T cr = wr ? r_sqrt_pos(h_r * GRAVITY) : Z;
-  const T un_l = wl ? dv(qn_l, h_l) : Z;
-  const T un_r = wr ? dv(qn_r, h_r) : Z;
+  const T un_l = wl ? dvp(qn_l, h_l) : Z;  // h > DRY_TOL > 0
+  const T un_r = wr ? dvp(qn_r, h_r) : Z;
   T sl, sr;
   if (wl && wr) {
     sl = r_min(un_l - cl, un_r - cr);
@@ -124,7 +124,7 @@ __device__ __forceinline__ void hllc_normal(T h_l, T qn_l, T qt_l, T h_r, T qn_r
   const T qt = left ? qt_l : qt_r;
   const T un = left ? un_l : un_r;
   const bool wet = left ? wl : wr;
-  const T ut = wet ? dv(qt, h) : Z;
+  const T ut = wet ? dvp(qt, h) : Z;
   T fm = Z, fn = Z, ft = Z;
   if (wet) {
     fm = qn;
@@ -156,12 +156,12 @@ __device__ __forceinline__ void wb_face(T hL, T qnL, T qtL, T hR, T qnR, T qtR, 
   const T hsR = r_max(hR + zf - z_max, Z);
   T unL = Z, utL = Z, unR = Z, utR = Z;
   if (val(hL) > H_VEL) {
-    unL = dv(qnL, hL);
-    utL = dv(qtL, hL);
+    unL = dvp(qnL, hL);  // hL > H_VEL
+    utL = dvp(qtL, hL);
   }
   if (val(hR) > H_VEL) {
-    unR = dv(qnR, hR);
-    utR = dv(qtR, hR);
+    unR = dvp(qnR, hR);
+    utR = dvp(qtR, hR);
   }
   T fm, fn, ft;
   hllc_normal<T>(hsL, hsL * unL, hsL * utL, hsR, hsR * unR, hsR * utR, fm, fn, ft);
@@ -175,7 +175,7 @@ __device__ __forceinline__ void wb_face(T hL, T qnL, T qtL, T hR, T qnR, T qtR, 
 
 // The reference's minmod(dl / d, dr / d) evaluated literally (update.rs:362-370).
 template <class T> __device__ __noinline__ T minmod_literal(T dl, T dr, double d) {
-  const T a = dv(dl, d), b = dv(dr, d);
+  const T a = dvp(dl, d), b = dvp(dr, d);  // d = dx or dy > 0
   if (val(a) * val(b) <= 0.0) return cst<T>(0.0);
   return fabs(val(a)) < fabs(val(b)) ? a : b;
 }
@@ -192,7 +192,7 @@ template <class T> __device__ __forceinline__ T minmod_div(T dl, T dr, double d)
   if ((hfa::is_zero(l) || hfa::is_zero(r)) && finite) return cst<T>(0.0);
   if (!finite || fabs(l) < 1.0e-140 || fabs(r) < 1.0e-140) return minmod_literal<T>(dl, dr, d);
   if (l * r <= 0.0) return cst<T>(0.0);
-  return dv(fabs(l) < fabs(r) ? dl : dr, d);
+  return dvp(fabs(l) < fabs(r) ? dl : dr, d);
 }
 
 // Which operand minmod_div(dl, dr, d) returns: -1 for the constant zero, 0

@@ -101,6 +101,9 @@ extern "C" int hf_ssprk2_step_noalloc(const hf_grid* grid, double* h, double* hu
     return noalloc_fail(HF_ERR_INVALID_ARG, buf);
   }
   if (device < 0 || device >= 64) return noalloc_fail(HF_ERR_INVALID_ARG, "bad device index");
+  // Mesh2D's own checks (geometry.rs:59, 93: dx, dy strictly positive).
+  if (!(grid->dx > 0.0) || !(grid->dy > 0.0))
+    return noalloc_fail(HF_ERR_INVALID_ARG, "dx and dy must be strictly positive");
   hf_boundary t{HF_BC_TRANSMISSIVE, 0, 0.0};
   const hf_boundaries b = bcs ? *bcs : hf_boundaries{t, t, t, t};
   const hf_boundary* sides[4] = {&b.north, &b.south, &b.west, &b.east};

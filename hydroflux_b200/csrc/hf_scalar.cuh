@@ -56,6 +56,20 @@ __device__ __forceinline__ DualD dv(double a, DualD b) {
   return DualD{hfa::div_rn(a, b.v), hfa::div_rn(-a * b.d, b.v * b.v)};
 }
 
+// Division by a divisor known to be > 0 (see hfa::div_rn_pos); the
+// derivative parts whose divisor is b^2 (which can underflow to 0) keep the
+// general division.
+__device__ __forceinline__ double dvp(double a, double b) { return hfa::div_rn_pos(a, b); }
+__device__ __forceinline__ DualD dvp(DualD a, DualD b) {
+  return DualD{hfa::div_rn_pos(a.v, b.v), hfa::div_rn(a.d * b.v - a.v * b.d, b.v * b.v)};
+}
+__device__ __forceinline__ DualD dvp(DualD a, double b) {
+  return DualD{hfa::div_rn_pos(a.v, b), hfa::div_rn_pos(a.d, b)};
+}
+__device__ __forceinline__ DualD dvp(double a, DualD b) {
+  return DualD{hfa::div_rn_pos(a, b.v), hfa::div_rn(-a * b.d, b.v * b.v)};
+}
+
 // sqrt (dual.rs:46-50): derivative 0 where the root is 0.
 __device__ __forceinline__ double r_sqrt(double x) { return hfa::sqrt_rn(x); }
 __device__ __forceinline__ DualD r_sqrt(DualD x) {

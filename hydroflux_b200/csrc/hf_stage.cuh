@@ -236,8 +236,8 @@ __device__ __forceinline__ void stage_tile_faces(const StageArgs& A, StageSmemT<
           zz = A.z[g];
           e = hh + zz;
           if (val(hh) > H_VEL) {
-            uu = dv(Field<T>::ld(A.in_hu, A.tan.in_hu, g), hh);
-            vv = dv(Field<T>::ld(A.in_hv, A.tan.in_hv, g), hh);
+            uu = dvp(Field<T>::ld(A.in_hu, A.tan.in_hu, g), hh);  // hh > H_VEL
+            vv = dvp(Field<T>::ld(A.in_hv, A.tan.in_hv, g), hh);
           }
         }
         S.z[k3] = zz;
@@ -279,14 +279,14 @@ __device__ __forceinline__ void stage_tile_faces(const StageArgs& A, StageSmemT<
           const int c3 = i3(li, lj);
           if (ga == 0) {
             const int r3 = c3 + st3;
-            se = dv(S.eta[r3] - S.eta[c3], d);
-            su = dv(S.u[r3] - S.u[c3], d);
-            sv = dv(S.v[r3] - S.v[c3], d);
+            se = dvp(S.eta[r3] - S.eta[c3], d);  // d = dx or dy > 0
+            su = dvp(S.u[r3] - S.u[c3], d);
+            sv = dvp(S.v[r3] - S.v[c3], d);
           } else if (ga == na - 1) {
             const int l3 = c3 - st3;
-            se = dv(S.eta[c3] - S.eta[l3], d);
-            su = dv(S.u[c3] - S.u[l3], d);
-            sv = dv(S.v[c3] - S.v[l3], d);
+            se = dvp(S.eta[c3] - S.eta[l3], d);
+            su = dvp(S.u[c3] - S.u[l3], d);
+            sv = dvp(S.v[c3] - S.v[l3], d);
           } else {
             const int l3 = c3 - st3, r3 = c3 + st3;
             se = minmod_div<T>(S.eta[c3] - S.eta[l3], S.eta[r3] - S.eta[c3], d);
@@ -417,7 +417,7 @@ __device__ __forceinline__ void stage_tile_faces(const StageArgs& A, StageSmemT<
       if (val(fb) > 0.0) out = out + fb * dt_dy;
       if (val(ft) < 0.0) out = out + (-ft) * dt_dy;
       const T avail = r_max(S.h[i4(li, lj)] - H_DRY, Z);
-      S.a[k] = (val(out) > val(avail) && val(out) > 0.0) ? dv(avail, out) : cst<T>(1.0);
+      S.a[k] = (val(out) > val(avail) && val(out) > 0.0) ? dvp(avail, out) : cst<T>(1.0);
     }
     __syncthreads();
   }
@@ -521,13 +521,13 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, StageSmemT<T>& S,
         const T eta_right = gj + 1 < nc ? eta_cell + sex * (0.5 * dx) : eta_cell;
         const T hfl = r_max(eta_left - zfl, Z);
         const T hfr = r_max(eta_right - zfr, Z);
-        const T s_hu = dv((hfl + hfr) * ((eta_left - hfl) - (eta_right - hfr)) * (0.5 * GRAVITY), dx);
+        const T s_hu = dvp((hfl + hfr) * ((eta_left - hfl) - (eta_right - hfr)) * (0.5 * GRAVITY), dx);
         const T sey = S.sye[isy(li, lj)];
         const T eta_top = gi > 0 ? eta_cell - sey * (0.5 * dy) : eta_cell;
         const T eta_bot = gi + 1 < nr ? eta_cell + sey * (0.5 * dy) : eta_cell;
         const T hft = r_max(eta_top - zft, Z);
         const T hfb = r_max(eta_bot - zfb, Z);
-        const T s_hv = dv((hft + hfb) * ((eta_top - hft) - (eta_bot - hfb)) * (0.5 * GRAVITY), dy);
+        const T s_hv = dvp((hft + hfb) * ((eta_top - hft) - (eta_bot - hfb)) * (0.5 * GRAVITY), dy);
 
         if (val(new_h) <= H_VEL) {
           nh = r_max(new_h, Z);  // moisture floor keeps the mass
