@@ -390,6 +390,8 @@ def run_ensemble(a, d: Dist):
     cells = np.array([s.n_cells for s in mine], dtype=np.float64)
     ens = Ensemble(mine, device=dev)
     ens.run(max(a.warmup, 3))
+    ens.run(64)  # untimed: the tile-schedule autotuner times 2 x 4 chunks of 8 steps
+    sched, tune_ms = ens.schedule()
     st0 = np.array([ens.info(k)["steps"] for k in range(len(mine))], dtype=np.float64)
     torch.cuda.synchronize(dev)
     d.barrier()
@@ -440,6 +442,9 @@ def run_ensemble(a, d: Dist):
                                      "scenarios_timed": len(sub)},
             "speedup_vs_loop": (batched_rate / d.world) / loop_rate if loop_rate else None,
             "gpu_launches": 4 * a.steps, "generation_s": gen_s, "complete": complete,
+            "schedule": {"chosen": Ensemble.SCHEDULES.get(sched, "untuned"),
+                         "tuning_ms_per_candidate": [float(x) for x in tune_ms],
+                         "autotune_steps": 64},
             "clocks": clk}
     if d.rank == 0:
         print(json.dumps(line), flush=True)

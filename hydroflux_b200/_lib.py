@@ -58,6 +58,8 @@ PROTOTYPES = {
     "hf_batch_scenario_info": (C.c_int, [_VP, C.c_int64, _D, C.POINTER(C.c_uint64),
                                          C.POINTER(C.c_int)]),
     "hf_batch_get_state": (C.c_int, [_VP, C.c_int64, _VP, _VP, _VP]),
+    "hf_batch_set_schedule": (C.c_int, [_VP, C.c_int]),
+    "hf_batch_schedule": (C.c_int, [_VP, C.POINTER(C.c_int), _D]),
     "hf_server_create": (C.c_int, [C.c_int, C.c_uint64, C.c_int, C.POINTER(_VP)]),
     "hf_server_destroy": (C.c_int, [_VP]),
     "hf_server_admit": (C.c_int, [_VP, C.POINTER(abi.hf_scenario_desc), C.POINTER(C.c_int)]),

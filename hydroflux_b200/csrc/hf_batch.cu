@@ -7,6 +7,14 @@
 // 64 batch steps. A small scenario no longer leaves most of the GPU idle or
 // pays a launch per step: the persistent grid keeps every SM busy with tiles
 // from whichever scenarios are still running.
+//
+// Schedules. How the CTAs walk the tile list is chosen by an online
+// autotuner, since the best choice depends on the mix (sizes, wet fraction,
+// horizons): {static stride, dynamic (atomic tile counter)} x {scenario
+// order, largest scenarios first}. The first hf_batch_run with enough steps
+// runs two rounds of 8-step graph chunks, one chunk per candidate in turn,
+// timed with CUDA events, and keeps the fastest candidate. Tuning steps are
+// real steps: the schedule changes no result.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -57,6 +65,7 @@ struct Guard {
 };
 
 const int kBatchChunk[3] = {1, 8, 64};
+constexpr int kSchedules = 4;  // bit 0: dynamic; bit 1: largest scenarios first
 
 }  // namespace
 
@@ -79,7 +88,15 @@ struct hf_batch {
   std::vector<ForcingHost> forcing;
   std::vector<int64_t> off, nr, nc;
   std::vector<double> t_end;
-  cudaGraphExec_t graphs[3] = {nullptr, nullptr, nullptr};
+  // schedule tables: order 1 lists the scenarios largest first
+  int* d_tile_scn_lpt = nullptr;
+  int* d_tile_local = nullptr;      // tile index within its scenario, order 0
+  int* d_tile_local_lpt = nullptr;  // order 1
+  int* d_counters = nullptr;        // dynamic schedule: stage 1 / stage 2 tile counters
+  cudaGraphExec_t graphs[kSchedules][3] = {};
+  int schedule = -1;  // -1: not tuned yet
+  int forced = -1;    // hf_batch_set_schedule
+  double tune_ms[kSchedules] = {0.0, 0.0, 0.0, 0.0};
 };
 
 namespace {
@@ -88,43 +105,51 @@ void destroy_batch(hf_batch* b) {
   if (!b) return;
   Guard g(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
-  for (auto& ge : b->graphs)
-    if (ge) cudaGraphExecDestroy(ge);
+  for (auto& row : b->graphs)
+    for (auto& ge : row)
+      if (ge) cudaGraphExecDestroy(ge);
   for (auto& f : b->forcing) {
     f.release_rain();
     f.release_src();
   }
   for (void* p : {(void*)b->buf, (void*)b->d_ctrl, (void*)b->d_args1, (void*)b->d_args2,
-                  (void*)b->d_tile_scn, (void*)b->d_n_tiles})
+                  (void*)b->d_tile_scn, (void*)b->d_n_tiles, (void*)b->d_tile_scn_lpt,
+                  (void*)b->d_tile_local, (void*)b->d_tile_local_lpt, (void*)b->d_counters})
     if (p) cudaFree(p);
   if (b->h_ctrl) cudaFreeHost(b->h_ctrl);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
 }
 
-int enqueue_batch_step(hf_batch* b) {
-  if (launch_batch_control(b->d_ctrl, b->d_args1, b->n, b->stream)) return bcuda(cudaGetLastError(), "control");
-  if (launch_stage_batch(b->d_args1, b->d_tile_scn, b->d_n_tiles, b->grid, b->stream))
+int enqueue_batch_step(hf_batch* b, int sched) {
+  const bool dynamic = sched & 1, lpt = sched & 2;
+  const int* scn = lpt ? b->d_tile_scn_lpt : b->d_tile_scn;
+  const int* local = lpt ? b->d_tile_local_lpt : (dynamic ? b->d_tile_local : nullptr);
+  int* c1 = dynamic ? b->d_counters : nullptr;
+  int* c2 = dynamic ? b->d_counters + 1 : nullptr;
+  if (launch_batch_control(b->d_ctrl, b->d_args1, b->n, b->stream, dynamic ? b->d_counters : nullptr))
+    return bcuda(cudaGetLastError(), "control");
+  if (launch_stage_batch(b->d_args1, scn, b->d_n_tiles, b->grid, b->stream, local, c1))
     return bcuda(cudaGetLastError(), "stage 1");
-  if (launch_stage_batch(b->d_args2, b->d_tile_scn, b->d_n_tiles, b->grid, b->stream))
+  if (launch_stage_batch(b->d_args2, scn, b->d_n_tiles, b->grid, b->stream, local, c2))
     return bcuda(cudaGetLastError(), "stage 2");
   if (launch_batch_commit(b->d_ctrl, b->n, b->stream)) return bcuda(cudaGetLastError(), "commit");
   return HF_OK;
 }
 
-int build_batch_graph(hf_batch* b, int which) {
-  if (b->graphs[which]) return HF_OK;
+int build_batch_graph(hf_batch* b, int sched, int which) {
+  if (b->graphs[sched][which]) return HF_OK;
   cudaGraph_t graph = nullptr;
   B_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
   int rc = HF_OK;
-  for (int k = 0; k < kBatchChunk[which] && rc == HF_OK; ++k) rc = enqueue_batch_step(b);
+  for (int k = 0; k < kBatchChunk[which] && rc == HF_OK; ++k) rc = enqueue_batch_step(b, sched);
   cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
   if (rc != HF_OK) {
     if (graph) cudaGraphDestroy(graph);
     return rc;
   }
   B_CUDA(e);
-  e = cudaGraphInstantiate(&b->graphs[which], graph, 0);
+  e = cudaGraphInstantiate(&b->graphs[sched][which], graph, 0);
   cudaGraphDestroy(graph);
   B_CUDA(e);
   return HF_OK;
@@ -141,6 +166,32 @@ int64_t count_unfinished(const hf_batch* b) {
   for (int s = 0; s < b->n; ++s)
     if (b->h_ctrl[s].status == 0 && b->h_ctrl[s].t < b->t_end[s]) ++k;
   return k;
+}
+
+// One graph chunk of schedule `sched`, then the control blocks read back.
+// elapsed_ms (optional): device time of the chunk.
+int run_chunk(hf_batch* b, int sched, int which, int64_t* running, float* elapsed_ms) {
+  const long long steps_before = total_steps(b);
+  B_TRY(build_batch_graph(b, sched, which));
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (elapsed_ms) {
+    B_CUDA(cudaEventCreate(&e0));
+    B_CUDA(cudaEventCreate(&e1));
+    B_CUDA(cudaEventRecord(e0, b->stream));
+  }
+  B_CUDA(cudaGraphLaunch(b->graphs[sched][which], b->stream));
+  if (elapsed_ms) B_CUDA(cudaEventRecord(e1, b->stream));
+  B_CUDA(cudaMemcpyAsync(b->h_ctrl, b->d_ctrl, b->n * sizeof(Ctrl), cudaMemcpyDeviceToHost, b->stream));
+  B_CUDA(cudaStreamSynchronize(b->stream));
+  if (elapsed_ms) {
+    cudaEventElapsedTime(elapsed_ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+  *running = count_unfinished(b);
+  if (*running > 0 && total_steps(b) == steps_before)  // would repeat forever
+    return bfail(HF_ERR_TIMEOUT, "ensemble made no progress: no scenario took a step");
+  return HF_OK;
 }
 
 }  // namespace
@@ -200,11 +251,15 @@ int hf_batch_create(int64_t n_scenarios, const hf_scenario_desc* sc, int device,
       cudaMalloc((void**)&b->d_args1, b->n * sizeof(StageArgs)) != cudaSuccess ||
       cudaMalloc((void**)&b->d_args2, b->n * sizeof(StageArgs)) != cudaSuccess ||
       cudaMalloc((void**)&b->d_tile_scn, b->total_tiles * sizeof(int)) != cudaSuccess ||
+      cudaMalloc((void**)&b->d_tile_scn_lpt, b->total_tiles * sizeof(int)) != cudaSuccess ||
+      cudaMalloc((void**)&b->d_tile_local, b->total_tiles * sizeof(int)) != cudaSuccess ||
+      cudaMalloc((void**)&b->d_tile_local_lpt, b->total_tiles * sizeof(int)) != cudaSuccess ||
+      cudaMalloc((void**)&b->d_counters, 2 * sizeof(int)) != cudaSuccess ||
       cudaMalloc((void**)&b->d_n_tiles, sizeof(int)) != cudaSuccess ||
       cudaMallocHost((void**)&b->h_ctrl, b->n * sizeof(Ctrl)) != cudaSuccess)
     return done(bcuda(cudaGetLastError(), "cudaMalloc(ensemble tables)"));
   std::vector<StageArgs> a1(b->n), a2(b->n);
-  std::vector<int> tile_scn(b->total_tiles);
+  std::vector<int> tile_scn(b->total_tiles), tile_local(b->total_tiles);
   std::memset(b->h_ctrl, 0, b->n * sizeof(Ctrl));
   int64_t o = 0;
   int tb = 0;
@@ -267,13 +322,33 @@ int hf_batch_create(int64_t n_scenarios, const hf_scenario_desc* sc, int device,
     y.combine = 1;
     y.finalize = 1;
     a2[s] = y;
-    for (int t = 0; t < tx * ty; ++t) tile_scn[tb + t] = s;
+    for (int t = 0; t < tx * ty; ++t) {
+      tile_scn[tb + t] = s;
+      tile_local[tb + t] = t;
+    }
     tb += tx * ty;
     o += ncell;
   }
+  // Order 1: the same tiles, scenarios by decreasing tile count (stable).
+  std::vector<int> by_size(b->n), tile_scn_lpt, tile_local_lpt;
+  for (int s = 0; s < b->n; ++s) by_size[s] = s;
+  std::stable_sort(by_size.begin(), by_size.end(), [&](int x, int y) {
+    return a1[x].tiles_x * a1[x].tiles_y > a1[y].tiles_x * a1[y].tiles_y;
+  });
+  tile_scn_lpt.reserve(b->total_tiles);
+  tile_local_lpt.reserve(b->total_tiles);
+  for (int s : by_size)
+    for (int t = 0; t < a1[s].tiles_x * a1[s].tiles_y; ++t) {
+      tile_scn_lpt.push_back(s);
+      tile_local_lpt.push_back(t);
+    }
   if (cudaMemcpy(b->d_args1, a1.data(), b->n * sizeof(StageArgs), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(b->d_args2, a2.data(), b->n * sizeof(StageArgs), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(b->d_tile_scn, tile_scn.data(), b->total_tiles * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(b->d_tile_local, tile_local.data(), b->total_tiles * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(b->d_tile_scn_lpt, tile_scn_lpt.data(), b->total_tiles * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(b->d_tile_local_lpt, tile_local_lpt.data(), b->total_tiles * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemset(b->d_counters, 0, 2 * sizeof(int)) != cudaSuccess ||
       cudaMemcpy(b->d_n_tiles, &b->total_tiles, sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(b->d_ctrl, b->h_ctrl, b->n * sizeof(Ctrl), cudaMemcpyHostToDevice) != cudaSuccess)
     return done(bcuda(cudaGetLastError(), "upload ensemble tables"));
@@ -298,19 +373,57 @@ int hf_batch_run(hf_batch* b, uint64_t max_batch_steps, int64_t* n_unfinished) {
   B_CUDA(cudaMemcpyAsync(b->h_ctrl, b->d_ctrl, b->n * sizeof(Ctrl), cudaMemcpyDeviceToHost, b->stream));
   B_CUDA(cudaStreamSynchronize(b->stream));
   int64_t running = count_unfinished(b);
+  if (b->schedule < 0 && b->forced >= 0) b->schedule = b->forced;
+  if (b->schedule < 0 && left >= (uint64_t)(2 * kSchedules * kBatchChunk[1]) && running > 0) {
+    // Autotune: two rounds of one 8-step chunk per candidate, alternating so
+    // that the flow's slow change over the rounds weighs on all of them.
+    double ms[kSchedules] = {0.0, 0.0, 0.0, 0.0};
+    int done_rounds = 0;
+    for (int r = 0; r < 2 && running > 0; ++r) {
+      double round_ms[kSchedules] = {0.0, 0.0, 0.0, 0.0};
+      int ran = 0;
+      for (int c = 0; c < kSchedules && running > 0; ++c, ++ran) {
+        float el = 0.f;
+        B_TRY(run_chunk(b, c, 1, &running, &el));
+        left -= (uint64_t)kBatchChunk[1];
+        round_ms[c] = el;
+      }
+      if (ran < kSchedules) break;  // the ensemble finished inside the round
+      for (int c = 0; c < kSchedules; ++c) ms[c] += round_ms[c];
+      ++done_rounds;
+    }
+    if (done_rounds > 0) {
+      int best = 0;
+      for (int c = 1; c < kSchedules; ++c)
+        if (ms[c] < ms[best]) best = c;
+      b->schedule = best;
+      for (int c = 0; c < kSchedules; ++c) b->tune_ms[c] = ms[c];
+    }
+  }
+  const int sched = b->schedule >= 0 ? b->schedule : 0;
   while (left > 0 && running > 0) {
     const int which = left >= 64 ? 2 : (left >= 8 ? 1 : 0);
-    const long long steps_before = total_steps(b);
-    B_TRY(build_batch_graph(b, which));
-    B_CUDA(cudaGraphLaunch(b->graphs[which], b->stream));
+    B_TRY(run_chunk(b, sched, which, &running, nullptr));
     left -= (uint64_t)kBatchChunk[which];
-    B_CUDA(cudaMemcpyAsync(b->h_ctrl, b->d_ctrl, b->n * sizeof(Ctrl), cudaMemcpyDeviceToHost, b->stream));
-    B_CUDA(cudaStreamSynchronize(b->stream));
-    running = count_unfinished(b);
-    if (running > 0 && total_steps(b) == steps_before)  // would repeat forever
-      return bfail(HF_ERR_TIMEOUT, "ensemble made no progress: no scenario took a step");
   }
   if (n_unfinished) *n_unfinished = running;
+  return HF_OK;
+}
+
+int hf_batch_set_schedule(hf_batch* b, int schedule) {
+  if (!b) return bfail(HF_ERR_INVALID_ARG, "null handle");
+  if (schedule < -1 || schedule >= kSchedules)
+    return bfail(HF_ERR_INVALID_ARG, "schedule must be -1 (autotune) or 0..3");
+  b->forced = schedule;
+  b->schedule = schedule;
+  return HF_OK;
+}
+
+int hf_batch_schedule(const hf_batch* b, int* schedule, double* tune_ms) {
+  if (!b) return bfail(HF_ERR_INVALID_ARG, "null handle");
+  if (schedule) *schedule = b->schedule;
+  if (tune_ms)
+    for (int c = 0; c < kSchedules; ++c) tune_ms[c] = b->tune_ms[c];
   return HF_OK;
 }
 

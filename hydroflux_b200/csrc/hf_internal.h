@@ -255,11 +255,15 @@ int forcing_set_sources(ForcingHost& f, int64_t nr, int64_t nc, int tiles_x, int
 // arrays of stage-1 / stage-2 arguments, ctrls the per-scenario control blocks.
 // n_tiles is a device int (the tile list length, read at launch time); the
 // CFL reduction covers tiles [first_tile, last_tile).
+// tile_local / counter select the schedule (see k_stage_batch); the defaults
+// are the static stride over scenario-contiguous tiles.
 int launch_stage_batch(const StageArgs* args, const int* tile_scn, const int* n_tiles, int grid,
-                       void* stream);
+                       void* stream, const int* tile_local = nullptr, int* counter = nullptr);
 int launch_cfl_batch(const StageArgs* args, const int* tile_scn, int first_tile, int last_tile,
                      int grid, void* stream);
-int launch_batch_control(Ctrl* ctrls, const StageArgs* args, int n, void* stream);
+// counters (2 ints, may be NULL) are zeroed for the dynamic schedule.
+int launch_batch_control(Ctrl* ctrls, const StageArgs* args, int n, void* stream,
+                         int* counters = nullptr);
 int launch_batch_commit(Ctrl* ctrls, int n, void* stream);
 
 }  // namespace hf

@@ -109,19 +109,46 @@ __global__ void __launch_bounds__(NTHREADS, HF_MIN_BLOCKS) k_stage_pf(const Stag
 // block) are args[tile_scn[t]]. Finished scenarios' tiles are skipped. The
 // CFL maxima are reduced per tile into the tile's scenario; each scenario's
 // clock is committed afterwards by k_batch_commit.
+//
+// Schedules (the ensemble's autotuner picks one): tile_local == nullptr
+// means tile t is tile t - tile_base of its scenario, else tile_local[t]
+// (any order of the list); counter == nullptr strides the list statically
+// (tile blockIdx.x, + gridDim.x, ...), else CTAs take the next tile from the
+// counter (dynamic; k_batch_control zeroes it before each step). Results do
+// not depend on the schedule: tiles are independent and the CFL reduction is
+// a max.
+__device__ __forceinline__ void batch_tile(const StageArgs* __restrict__ args,
+                                           const int* __restrict__ tile_scn,
+                                           const int* __restrict__ tile_local, int t,
+                                           StageSmem& S) {
+  const StageArgs& A = args[tile_scn[t]];
+  if (!A.ctrl->active) return;  // uniform over the CTA
+  double sxm = 0.0, sym = 0.0;
+  unsigned long long nonfin = 0;
+  stage_tile<double>(A, S, tile_local ? tile_local[t] : t - A.tile_base, sxm, sym, nonfin);
+  if (A.finalize) block_reduce_speeds(sxm, sym, nonfin, A.ctrl);
+}
+
 __global__ void __launch_bounds__(NTHREADS, HF_MIN_BLOCKS)
     k_stage_batch(const StageArgs* __restrict__ args, const int* __restrict__ tile_scn,
-                  const int* __restrict__ n_tiles) {
+                  const int* __restrict__ tile_local, const int* __restrict__ n_tiles,
+                  int* counter) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   StageSmem& S = *reinterpret_cast<StageSmem*>(smem_raw);
   const int total_tiles = *n_tiles;  // device-resident: a graph serves any set of scenarios
-  for (int t = blockIdx.x; t < total_tiles; t += gridDim.x) {
-    const StageArgs& A = args[tile_scn[t]];
-    if (!A.ctrl->active) continue;  // uniform over the CTA
-    double sxm = 0.0, sym = 0.0;
-    unsigned long long nonfin = 0;
-    stage_tile<double>(A, S, t - A.tile_base, sxm, sym, nonfin);
-    if (A.finalize) block_reduce_speeds(sxm, sym, nonfin, A.ctrl);
+  if (counter == nullptr) {
+    for (int t = blockIdx.x; t < total_tiles; t += gridDim.x)
+      batch_tile(args, tile_scn, tile_local, t, S);
+    return;
+  }
+  __shared__ int next_tile;
+  while (true) {
+    if (threadIdx.x == 0) next_tile = atomicAdd(counter, 1);
+    __syncthreads();
+    const int t = next_tile;
+    __syncthreads();  // every thread has read next_tile before thread 0 takes another
+    if (t >= total_tiles) break;
+    batch_tile(args, tile_scn, tile_local, t, S);
   }
 }
 
@@ -309,8 +336,13 @@ __global__ void k_gauges(const Ctrl* c, const double* __restrict__ h, GaugeDev g
 }
 
 // Per-scenario control of an ensemble: one thread per scenario.
-__global__ void k_batch_control(Ctrl* ctrls, const StageArgs* __restrict__ args, int n) {
+__global__ void k_batch_control(Ctrl* ctrls, const StageArgs* __restrict__ args, int n,
+                                int* counters) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (counters && s == 0) {  // the dynamic schedule's tile counters of this step's two stages
+    counters[0] = 0;
+    counters[1] = 0;
+  }
   if (s >= n) return;
   const StageArgs& A = args[s];
   if (control_step(&ctrls[s], A.dx, A.dy, A.f))
@@ -547,9 +579,9 @@ int launch_finalize_dual(const StageArgs& a, int grid, void* stream, int lanes) 
 }
 
 int launch_stage_batch(const StageArgs* args, const int* tile_scn, const int* n_tiles, int grid,
-                       void* stream) {
-  k_stage_batch<<<grid, NTHREADS, sizeof(StageSmem), (cudaStream_t)stream>>>(args, tile_scn,
-                                                                             n_tiles);
+                       void* stream, const int* tile_local, int* counter) {
+  k_stage_batch<<<grid, NTHREADS, sizeof(StageSmem), (cudaStream_t)stream>>>(
+      args, tile_scn, tile_local, n_tiles, counter);
   return cuda_rc(cudaGetLastError());
 }
 
@@ -560,8 +592,9 @@ int launch_cfl_batch(const StageArgs* args, const int* tile_scn, int first_tile,
   return cuda_rc(cudaGetLastError());
 }
 
-int launch_batch_control(Ctrl* ctrls, const StageArgs* args, int n, void* stream) {
-  k_batch_control<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(ctrls, args, n);
+int launch_batch_control(Ctrl* ctrls, const StageArgs* args, int n, void* stream,
+                         int* counters) {
+  k_batch_control<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(ctrls, args, n, counters);
   return cuda_rc(cudaGetLastError());
 }
 

@@ -81,6 +81,22 @@ class Ensemble:
         raise_for(lib().hf_batch_run(self._h, int(max_batch_steps), C.byref(left)))
         return left.value
 
+    SCHEDULES = {0: "static, scenario order", 1: "dynamic, scenario order",
+                 2: "static, largest first", 3: "dynamic, largest first"}
+
+    def set_schedule(self, schedule: int = -1) -> None:
+        """Tile schedule of the batched kernel (-1: autotune on the first
+        run of >= 64 steps); no schedule changes any result."""
+        raise_for(lib().hf_batch_set_schedule(self._h, int(schedule)))
+
+    def schedule(self):
+        """(schedule in use, -1 before tuning; per-candidate tuning ms)."""
+        sc = C.c_int()
+        ms = np.zeros(4)
+        raise_for(lib().hf_batch_schedule(self._h, C.byref(sc), ms.ctypes.data_as(
+            C.POINTER(C.c_double))))
+        return sc.value, ms
+
     def info(self, k: int):
         t, st, status = C.c_double(), C.c_uint64(), C.c_int()
         raise_for(lib().hf_batch_scenario_info(self._h, int(k), C.byref(t), C.byref(st),

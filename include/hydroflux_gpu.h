@@ -235,6 +235,16 @@ int hf_batch_scenario_info(const hf_batch* batch, int64_t k, double* t, uint64_t
                            int* status);
 /* Host copy of scenario k's state. */
 int hf_batch_get_state(hf_batch* batch, int64_t k, double* h, double* hu, double* hv);
+/* Tile schedule of the batched stage kernel. 0: static stride over the tiles
+ * in scenario order; 1: dynamic (CTAs take the next tile from an atomic
+ * counter); 2 / 3: the same with the scenarios largest first. -1 (default):
+ * the first hf_batch_run with at least 64 steps times two 8-step chunks of
+ * each and keeps the fastest (those are real steps). No schedule changes any
+ * result. */
+int hf_batch_set_schedule(hf_batch* batch, int schedule);
+/* The schedule in use (-1 before tuning) and, after tuning, the measured
+ * milliseconds of each candidate's two chunks (tune_ms[4], may be NULL). */
+int hf_batch_schedule(const hf_batch* batch, int* schedule, double* tune_ms);
 
 /* ---------------------------------------------------------------------------
  * Serving: continuous batching of flood scenarios on one GPU. No counterpart

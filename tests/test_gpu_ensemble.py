@@ -88,3 +88,38 @@ def test_ensemble_partial_runs_and_failure_isolation(gpu):
         for k in range(3):
             info = ens.info(k)
             assert info["status"] == abi.HF_ERR_STEP_BUDGET and info["steps"] == 5
+
+
+@pytest.mark.parametrize("schedule", [0, 1, 2, 3])
+def test_every_schedule_gives_the_same_results(gpu, schedule):
+    """The autotuner's candidates (static / dynamic tile order, scenario order
+    / largest first) all give each scenario its lone solve, bit for bit."""
+    ensemble, workloads = gpu
+    scns = mixed_scenarios(workloads)
+    with ensemble.Ensemble(scns) as ens:
+        ens.set_schedule(schedule)
+        assert ens.run() == 0
+        assert ens.schedule()[0] == schedule
+        for k, s in enumerate(scns):
+            ref, steps, t = solve_alone(workloads, s)
+            info = ens.info(k)
+            assert info["steps"] == steps and info["t"] == t
+            assert exact_fraction(ens.states(k), ref) == 1.0, f"scenario {k}"
+
+
+def test_autotuner_picks_a_schedule_and_changes_nothing(gpu):
+    ensemble, workloads = gpu
+    scns = mixed_scenarios(workloads)
+    with ensemble.Ensemble(scns) as ens:
+        assert ens.schedule()[0] == -1
+        assert ens.run(max_batch_steps=7) >= 0   # too short to tune: schedule 0
+        assert ens.schedule()[0] == -1
+        ens.run()
+        sched, ms = ens.schedule()
+        assert sched in (0, 1, 2, 3) and np.all(ms > 0.0)
+        assert ms[sched] == ms.min()
+        for k, s in enumerate(scns):
+            ref, _, _ = solve_alone(workloads, s)
+            assert exact_fraction(ens.states(k), ref) == 1.0, f"scenario {k}"
+        with pytest.raises(ValueError):
+            ens.set_schedule(4)
