@@ -691,6 +691,22 @@ __global__ void k_calib_pre(const Ctrl* c, double* dts, double* ts, long long ca
   ts[c->steps] = c->t;
 }
 
+// Checkpoint of the state before step c->steps when that is a multiple of
+// `every` (the first step included; nothing once the run has ended).
+__global__ void k_calib_ckpt(const Ctrl* c, const double* __restrict__ h,
+                             const double* __restrict__ hu, const double* __restrict__ hv,
+                             double* ckpt, long long every, long long cap, long long ncell) {
+  const long long s = c->steps;
+  if (s % every != 0 || s >= cap || (s > 0 && !c->active)) return;
+  double* dst = ckpt + (s / every) * 3 * ncell;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < ncell;
+       i += (long long)gridDim.x * blockDim.x) {
+    dst[i] = h[i];
+    dst[ncell + i] = hu[i];
+    dst[2 * ncell + i] = hv[i];
+  }
+}
+
 __global__ void k_calib_post(const Ctrl* c, const double* __restrict__ h,
                              const double* __restrict__ dh, const int64_t* __restrict__ cells,
                              int n_gauges, double* gauge_h, double* gauge_dh, long long cap,
@@ -778,6 +794,14 @@ int launch_calib_post(const Ctrl* c, const double* h, const double* dh, const in
   if (n_gauges <= 0) return 0;
   k_calib_post<<<1, 128, 0, (cudaStream_t)stream>>>(c, h, dh, cells, n_gauges, gauge_h, gauge_dh,
                                                     cap, lanes, lane_stride);
+  return cuda_rc(cudaGetLastError());
+}
+
+int launch_calib_ckpt(const Ctrl* c, const double* h, const double* hu, const double* hv,
+                      double* ckpt, long long every, long long cap, long long ncell,
+                      void* stream) {
+  k_calib_ckpt<<<elem_grid(ncell), 256, 0, (cudaStream_t)stream>>>(c, h, hu, hv, ckpt, every,
+                                                                    cap, ncell);
   return cuda_rc(cudaGetLastError());
 }
 

@@ -129,6 +129,8 @@ struct hf_calib {
   double* dnL = nullptr;
   double* gdhL = nullptr;                      // [lane][K][G]
   double* Ualt[3] = {nullptr, nullptr, nullptr};  // second value buffer (no in-place stage 2)
+  // forward runs replayed from CUDA graphs: [mode][checkpoints][1 / 8 / 64 steps]
+  cudaGraphExec_t fgraphs[3][2][3] = {};
 };
 
 namespace {
@@ -225,6 +227,43 @@ int status_of_run(hf_calib* c, int64_t* n_run) {
 // recorded), 1: replay of the recorded dt, 2: DualD tangent (dU holds the
 // initial tangent; CFL dt from values, recorded). With checkpoints the state
 // before every C-th step is stored.
+const int kFwdChunk[3] = {1, 8, 64};
+
+// The launches of one forward step (see forward_run).
+int enqueue_forward_step(hf_calib* c, int mode, bool checkpoints, const StageArgs& a1,
+                         const StageArgs& a2, const ForcingDev& fd) {
+  const bool replay = mode == 1, dual = mode == 2;
+  const bool ssp = c->cfg.integrator == HF_SSPRK2;
+  if (checkpoints)
+    C_TRY(launch_calib_ckpt(c->ctrl, c->U[0], c->U[1], c->U[2], c->ckpt, (long long)c->C,
+                            (long long)c->K, (long long)c->ncell, c->stream));
+  C_TRY(launch_control(c->ctrl, c->dx, c->dy, fd, c->stream));
+  if (!replay) C_TRY(launch_calib_pre(c->ctrl, c->dts, c->ts, (long long)c->K, c->stream));
+  if (dual) {
+    C_TRY(launch_stage_dual(a1, c->grid_dual, c->stream));
+    if (ssp)
+      C_TRY(launch_stage_dual(a2, c->grid_dual, c->stream));
+    else
+      C_TRY(launch_finalize_dual(a2, c->grid, c->stream));
+  } else {
+    C_TRY(launch_stage(a1, c->grid, c->stream));
+    if (ssp)
+      C_TRY(launch_stage(a2, c->grid, c->stream));
+    else
+      C_TRY(launch_finalize(a2, c->grid, c->stream));
+  }
+  C_TRY(launch_calib_post(c->ctrl, c->U[0], dual ? c->dU[0] : nullptr, c->cells, (int)c->G,
+                          c->gh, c->gdh, (long long)c->K, c->stream));
+  return HF_OK;
+}
+
+// One forward run from the initial state. mode 0: primal with CFL dt (dt
+// recorded), 1: replay of the recorded dt, 2: DualD tangent (dU holds the
+// initial tangent; CFL dt from values, recorded). With checkpoints the state
+// before every C-th step is stored. The steps run from CUDA graphs of 64, 8
+// and 1 steps (the buffers are fixed per problem, so a graph is captured
+// once per mode); the control block is read back between graphs, and the
+// launches stop once the run has ended.
 int forward_run(hf_calib* c, int mode, bool checkpoints, int64_t* n_run) {
   const size_t bytes = (size_t)c->ncell * sizeof(double);
   double* h0[3] = {c->h0, c->hu0, c->hv0};
@@ -243,29 +282,29 @@ int forward_run(hf_calib* c, int mode, bool checkpoints, int64_t* n_run) {
   }
   if (!replay) C_TRY(launch_cfl(a1, 1, c->grid, c->stream));
   const int64_t steps = replay ? c->last_run : c->K;
-  for (int64_t k = 0; k < steps; ++k) {
-    if (checkpoints && k % c->C == 0)
-      for (int f = 0; f < 3; ++f)
-        C_CUDA(cudaMemcpyAsync(slot(c->ckpt, k / c->C, f, c->ncell), c->U[f], bytes,
-                               cudaMemcpyDeviceToDevice, c->stream));
-    C_TRY(launch_control(c->ctrl, c->dx, c->dy, fd, c->stream));
-    if (!replay) C_TRY(launch_calib_pre(c->ctrl, c->dts, c->ts, (long long)c->K, c->stream));
-    if (dual) {
-      C_TRY(launch_stage_dual(a1, c->grid_dual, c->stream));
-      if (ssp)
-        C_TRY(launch_stage_dual(a2, c->grid_dual, c->stream));
-      else
-        C_TRY(launch_finalize_dual(a2, c->grid, c->stream));
-    } else {
-      C_TRY(launch_stage(a1, c->grid, c->stream));
-      if (ssp)
-        C_TRY(launch_stage(a2, c->grid, c->stream));
-      else
-        C_TRY(launch_finalize(a2, c->grid, c->stream));
+  int64_t k = 0;
+  while (k < steps) {
+    const int which = steps - k >= 64 ? 2 : (steps - k >= 8 ? 1 : 0);
+    cudaGraphExec_t& ge = c->fgraphs[mode][checkpoints ? 1 : 0][which];
+    if (!ge) {
+      cudaGraph_t graph = nullptr;
+      C_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+      int rc = HF_OK;
+      for (int i = 0; i < kFwdChunk[which] && rc == HF_OK; ++i)
+        rc = enqueue_forward_step(c, mode, checkpoints, a1, a2, fd);
+      cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+      if (rc != HF_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+      }
+      C_CUDA(e);
+      e = cudaGraphInstantiate(&ge, graph, 0);
+      cudaGraphDestroy(graph);
+      C_CUDA(e);
     }
-    C_TRY(launch_calib_post(c->ctrl, c->U[0], dual ? c->dU[0] : nullptr, c->cells, (int)c->G,
-                            c->gh, c->gdh, (long long)c->K, c->stream));
-    if ((k + 1) % 64 == 0 && k + 1 < steps) {  // stop launching once the run has ended
+    C_CUDA(cudaGraphLaunch(ge, c->stream));
+    k += kFwdChunk[which];
+    if (k < steps) {  // stop launching once the run has ended
       C_CUDA(cudaMemcpyAsync(c->h_ctrl, c->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost,
                              c->stream));
       C_CUDA(cudaStreamSynchronize(c->stream));
@@ -456,6 +495,10 @@ void destroy_calib(hf_calib* c) {
   Guard g(c->device);
   for (cudaStream_t s : {c->stream, c->s_rec, c->s_rev})
     if (s) cudaStreamSynchronize(s);
+  for (auto& m : c->fgraphs)
+    for (auto& k : m)
+      for (auto& g : k)
+        if (g) cudaGraphExecDestroy(g);
   c->forcing.release_rain();
   c->forcing.release_src();
   std::vector<void*> ptrs = {c->z,    c->n,    c->dn,   c->h0,   c->hu0,  c->hv0,  c->cells,

@@ -219,6 +219,10 @@ int launch_calib_post(const Ctrl* c, const double* h, const double* dh, const in
                       int n_gauges, double* gauge_h, double* gauge_dh, long long cap,
                       void* stream, int lanes = 1, long long lane_stride = 0);
 int launch_calib_rewind(Ctrl* c, const double* ts, long long k, void* stream);
+// State checkpoint before the current step when c->steps % every == 0.
+int launch_calib_ckpt(const Ctrl* c, const double* h, const double* hu, const double* hv,
+                      double* ckpt, long long every, long long cap, long long ncell,
+                      void* stream);
 
 // Sets the calling thread's hf_last_error() message and returns `code`.
 int record_error(int code, const char* msg);
