@@ -288,7 +288,9 @@ def run_ours(a, d: Dist):
                "readback_ms": 1e3 * (t_b - t_s),
                "note": "Simulation::new from pinned host arrays (bed, n, h, hu, hv), K x "
                        "Simulation::step through the C ABI (dt read back each step), "
-                       "states() to pinned host; copies, allocation and graph capture timed"}
+                       "states() to pinned host; copies, allocation (from the library's "
+                       "device pool, which keeps the memory of the destroyed timed-leg "
+                       "handle) and graph capture timed"}
 
     cpu = None
     if d.rank == 0 and d.world == 1 and not a.no_cpu_baseline:

@@ -13,6 +13,7 @@
 #include <cstddef>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -98,6 +99,53 @@ int dalloc(T** p, size_t n) {
   if (n == 0) n = 1;
   cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
   return cuda_fail(e, "cudaMalloc");
+}
+
+// The state fields of simulation handles come from one memory pool per
+// device that keeps freed memory mapped (release threshold: never), so a
+// handle created after another was destroyed reuses its memory instead of
+// asking the driver for fresh pages (measured: 5-600 ms for 1 GB of new
+// allocations, against under a millisecond from the pool).
+// hf_release_cached_memory returns the pool's unused memory.
+std::mutex g_pool_mu;
+cudaMemPool_t g_pool[64] = {};
+
+int state_pool(int device, cudaMemPool_t* out) {
+  if (device < 0 || device >= 64) return fail(HF_ERR_INVALID_ARG, "bad device index");
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  if (!g_pool[device]) {
+    cudaMemPoolProps props;
+    std::memset(&props, 0, sizeof props);
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t pool = nullptr;
+    cudaError_t e = cudaMemPoolCreate(&pool, &props);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemPoolCreate");
+    unsigned long long keep = ~0ull;
+    e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    if (e != cudaSuccess) {
+      cudaMemPoolDestroy(pool);
+      return cuda_fail(e, "cudaMemPoolSetAttribute");
+    }
+    g_pool[device] = pool;
+  }
+  *out = g_pool[device];
+  return HF_OK;
+}
+
+// n doubles from the device's state pool, in order on `stream`.
+int palloc(double** p, size_t n, int device, cudaStream_t stream) {
+  cudaMemPool_t pool = nullptr;
+  HF_TRY(state_pool(device, &pool));
+  if (n == 0) n = 1;
+  return cuda_fail(cudaMallocFromPoolAsync((void**)p, n * sizeof(double), pool, stream),
+                   "cudaMallocFromPoolAsync");
+}
+
+void pfree(void* p, cudaStream_t stream) {
+  if (p) cudaFreeAsync(p, stream);
 }
 
 void dfree(void* p) {
@@ -396,8 +444,10 @@ void destroy_sim(hf_sim* s) {
   s->forcing.release_src();
   release_gauges(s);
   for (void* p : {(void*)s->d_z, (void*)s->d_n, (void*)s->d_h, (void*)s->d_hu, (void*)s->d_hv,
-                  (void*)s->d_h1, (void*)s->d_hu1, (void*)s->d_hv1, (void*)s->d_ctrl})
-    dfree(p);
+                  (void*)s->d_h1, (void*)s->d_hu1, (void*)s->d_hv1})
+    pfree(p, s->stream);
+  dfree(s->d_ctrl);
+  if (s->stream) cudaStreamSynchronize(s->stream);  // the frees complete before the stream goes
   if (s->h_ctrl) cudaFreeHost(s->h_ctrl);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
@@ -468,7 +518,10 @@ int hf_sim_create(const hf_mesh_desc* mesh, const double* h, const double* hu, c
     return done(cuda_fail(cudaGetLastError(), "cudaStreamCreate"));
   double** bufs[8] = {&s->d_z, &s->d_n, &s->d_h, &s->d_hu, &s->d_hv, &s->d_h1, &s->d_hu1, &s->d_hv1};
   for (double** b : bufs)
-    if ((rc = dalloc(b, (size_t)ncell)) != HF_OK) return done(rc);
+    if ((rc = palloc(b, (size_t)ncell, device, s->stream)) != HF_OK) return done(rc);
+  // Stream-ordered allocations: usable from any stream once this completes.
+  if (cudaStreamSynchronize(s->stream) != cudaSuccess)
+    return done(cuda_fail(cudaGetLastError(), "pool allocation"));
   if ((rc = dalloc(&s->d_ctrl, 1)) != HF_OK) return done(rc);
   if (cudaMallocHost((void**)&s->h_ctrl, sizeof(Ctrl)) != cudaSuccess)
     return done(cuda_fail(cudaGetLastError(), "cudaMallocHost"));
@@ -846,6 +899,16 @@ int hf_sim_gauge_series(hf_sim* s, double* t, double* h, int64_t* n_stored, int6
   if (stored > 0 && h)
     HF_CUDA(cudaMemcpy(h, s->gauge.ser_h, (size_t)stored * s->gauge.n * sizeof(double),
                        cudaMemcpyDeviceToHost));
+  return HF_OK;
+}
+
+int hf_release_cached_memory(int device) {
+  if (device < 0 || device >= 64) return fail(HF_ERR_INVALID_ARG, "bad device index");
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  if (!g_pool[device]) return HF_OK;
+  DeviceGuard guard(device);
+  HF_CUDA(cudaDeviceSynchronize());
+  HF_CUDA(cudaMemPoolTrimTo(g_pool[device], 0));
   return HF_OK;
 }
 

@@ -209,8 +209,8 @@ __device__ __forceinline__ void stage_tile_faces(const StageArgs& A, StageSmemT<
         const double zz = S.eta[k3], qu = S.u[k3], qv = S.v[k3];
         double uu = 0.0, vv = 0.0;
         if (hh > H_VEL) {
-          uu = hfa::div_rn(qu, hh);
-          vv = hfa::div_rn(qv, hh);
+          uu = hfa::div_rn_pos(qu, hh);
+          vv = hfa::div_rn_pos(qv, hh);
         }
         S.z[k3] = zz;
         S.eta[k3] = hh + zz;

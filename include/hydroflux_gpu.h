@@ -156,6 +156,11 @@ int hf_sim_get_state_aos(hf_sim* sim, double* hhuhv);
 int hf_sim_set_state_aos(hf_sim* sim, const double* hhuhv);
 /* Simulation::set_boundaries (sim.rs:194-196). */
 int hf_sim_set_boundaries(hf_sim* sim, const hf_boundaries* bcs);
+/* The state fields of simulation handles come from a per-device memory pool
+ * that keeps the memory of destroyed handles for the next ones (no driver
+ * allocation on re-creation). This returns the pool's unused memory to the
+ * device. */
+int hf_release_cached_memory(int device);
 /* Details of the last HF_ERR_DEGENERATE_DT / HF_ERR_STEP_BUDGET (the fields
  * of SimError::DegenerateDt {dt,t,step} / StepBudgetExhausted {steps,t}). */
 int hf_sim_error_detail(const hf_sim* sim, double* dt, double* t, uint64_t* step);

@@ -331,3 +331,24 @@ def test_lake_at_rest_and_mass_on_gpu(gpu, oracle, bed):
         assert np.max(np.abs(got[1])) <= 1e-13 and np.max(np.abs(got[2])) <= 1e-13
         assert np.max(np.abs(got[0] + z - eta)) <= 1e-13
     assert abs(got[0].sum() - h.sum()) <= 1e-12 * h.sum()
+
+
+def test_state_pool_reuse_and_release(gpu):
+    """Handles created after others were destroyed reuse pooled memory and
+    compute the same; releasing the pool's cache leaves live handles intact."""
+    sim, _ = gpu
+    from hydroflux_b200._lib import lib
+    z, n, h, hu, hv = random_case(64, 96, 5)
+    results = []
+    live = sim.Simulation(sim.Mesh2D(z, 1.0, 1.0, n), (h, hu, hv))
+    for k in range(3):
+        with sim.Simulation(sim.Mesh2D(z, 1.0, 1.0, n), (h, hu, hv)) as s:
+            s.run_steps(20)
+            results.append(s.states())
+        if k == 1:
+            assert lib().hf_release_cached_memory(0) == 0
+    live.run_steps(20)
+    results.append(live.states())
+    live.close()
+    for r in results[1:]:
+        assert all(np.array_equal(a, b) for a, b in zip(r, results[0]))
