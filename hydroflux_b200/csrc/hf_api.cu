@@ -296,6 +296,8 @@ StageArgs stage_args(const hf_sim* s, bool second) {
   a.tiles_y = s->tiles_y;
   a.dx = s->dx;
   a.dy = s->dy;
+  a.rx = hfa::make_recip(a.dx);
+  a.ry = hfa::make_recip(a.dy);
   a.z = s->d_z;
   a.n = s->d_n;
   a.bc = to_bcdev(s->cfg.boundaries);
@@ -983,6 +985,8 @@ StageArgs ws_args(const hf_grid* g, const hf_boundaries& bcs, hf_workspace* w) {
   a.tiles_y = (int)((g->n_rows + TY - 1) / TY);
   a.dx = g->dx;
   a.dy = g->dy;
+  a.rx = hfa::make_recip(a.dx);
+  a.ry = hfa::make_recip(a.dy);
   a.z = g->bed;
   a.n = g->manning;
   a.bc = to_bcdev(bcs);

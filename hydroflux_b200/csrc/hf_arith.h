@@ -18,6 +18,7 @@
 
 #include <cmath>
 #include <cstdint>
+#include <cstring>
 
 #if defined(__CUDACC__)
 #define HF_ARITH_HD __host__ __device__ __forceinline__
@@ -26,6 +27,41 @@
 #endif
 
 namespace hfa {
+
+// Division by a fixed divisor d (a grid spacing) through its reciprocal,
+// correctly rounded like a / d (div_recip). Method: y = hi + lo is 1/d to
+// ~2^-105 (hi = RN(1/d), lo = RN((1 - d*hi) * hi), the residual being exact);
+// q0 = RN(a*hi + RN(a*lo)) is then within one ulp of a/d, so r = a - d*q0 is
+// exact in one fma and RN(q0 + r*hi) is RN(a/d) (Markstein's theorem:
+// P. Markstein, IBM J. Res. Dev. 34(1), 1990; J.-M. Muller et al., Handbook
+// of Floating-Point Arithmetic, "division with an FMA"). It holds without
+// underflow or overflow in the intermediates, so it is used only for d with
+// an exponent in [-100, 100] (ok) and a with one in [-700, 900]; everything
+// else (zeros, subnormals, infinities, NaN, extreme values) takes the IEEE
+// division. A default RecipD (ok = false) always divides. make_recip runs
+// on the host (kernel arguments) or the device with the same result.
+struct RecipD {
+  double d = 0.0, hi = 0.0, lo = 0.0;
+  bool ok = false;
+};
+HF_ARITH_HD int biased_exponent(double x) {
+#if defined(__CUDA_ARCH__)
+  const long long b = __double_as_longlong(x);
+#else
+  long long b;
+  std::memcpy(&b, &x, sizeof b);
+#endif
+  return (int)((b >> 52) & 0x7ff);
+}
+HF_ARITH_HD RecipD make_recip(double d) {
+  RecipD r;
+  r.d = d;
+  r.hi = 1.0 / d;
+  r.lo = fma(-d, r.hi, 1.0) * r.hi;
+  const int e = biased_exponent(d);
+  r.ok = d > 0.0 && e >= 1023 - 100 && e <= 1023 + 100;
+  return r;
+}
 
 #if defined(__CUDA_ARCH__)
 HF_ARITH_HD double div_rn(double a, double b) {
@@ -48,6 +84,13 @@ HF_ARITH_HD double div_rn_pos(double a, double b) {
   const double q = num / b;
   return a_zero ? a : q;
 }
+HF_ARITH_HD double div_recip(double a, const RecipD& r) {
+  const int e = biased_exponent(a);
+  if (!r.ok || e < 1023 - 700 || e > 1023 + 900) return div_rn_pos(a, r.d);
+  const double q0 = fma(a, r.hi, a * r.lo);
+  const double res = fma(-r.d, q0, a);
+  return fma(res, r.hi, q0);
+}
 HF_ARITH_HD double sqrt_rn(double x) {
   const bool zero = (__double_as_longlong(x) << 1) == 0;
   double y = zero ? 1.0 : x;
@@ -63,6 +106,7 @@ HF_ARITH_HD bool is_finite(double x) {
 #else
 HF_ARITH_HD double div_rn(double a, double b) { return a / b; }
 HF_ARITH_HD double div_rn_pos(double a, double b) { return a / b; }
+HF_ARITH_HD double div_recip(double a, const RecipD& r) { return a / r.d; }
 HF_ARITH_HD double sqrt_rn(double x) { return std::sqrt(x); }
 HF_ARITH_HD bool is_zero(double x) { return x == 0.0; }
 HF_ARITH_HD bool is_finite(double x) { return std::isfinite(x); }

@@ -306,6 +306,8 @@ int hf_batch_create(int64_t n_scenarios, const hf_scenario_desc* sc, int device,
     x.tile_base = tb;
     x.dx = d.mesh.dx;
     x.dy = d.mesh.dy;
+    x.rx = hfa::make_recip(x.dx);
+    x.ry = hfa::make_recip(x.dy);
     x.z = b->z + o;
     x.n = b->nman + o;
     x.bc = boundaries_dev(d.cfg.boundaries);

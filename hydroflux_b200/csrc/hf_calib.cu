@@ -147,6 +147,8 @@ StageArgs calib_args(const hf_calib* c, double* const in[3], double* const out[3
   a.pad_ = 0;
   a.dx = c->dx;
   a.dy = c->dy;
+  a.rx = hfa::make_recip(a.dx);
+  a.ry = hfa::make_recip(a.dy);
   a.z = c->z;
   a.n = c->n;
   a.in_h = in[0]; a.in_hu = in[1]; a.in_hv = in[2];

@@ -186,13 +186,13 @@ template <class T> __device__ __noinline__ T minmod_literal(T dl, T dr, double d
 // value). A zero difference makes the reference's product of quotients +-0,
 // hence 0. Tiny or infinite operands, where the reference's product of
 // quotients could underflow or be NaN, take the literal path out of line.
-template <class T> __device__ __forceinline__ T minmod_div(T dl, T dr, double d) {
+template <class T> __device__ __forceinline__ T minmod_div(T dl, T dr, const hfa::RecipD& rd) {
   const double l = val(dl), r = val(dr);
   const bool finite = hfa::is_finite(l) && hfa::is_finite(r);
   if ((hfa::is_zero(l) || hfa::is_zero(r)) && finite) return cst<T>(0.0);
-  if (!finite || fabs(l) < 1.0e-140 || fabs(r) < 1.0e-140) return minmod_literal<T>(dl, dr, d);
+  if (!finite || fabs(l) < 1.0e-140 || fabs(r) < 1.0e-140) return minmod_literal<T>(dl, dr, rd.d);
   if (l * r <= 0.0) return cst<T>(0.0);
-  return dvp(fabs(l) < fabs(r) ? dl : dr, d);
+  return dvr(fabs(l) < fabs(r) ? dl : dr, rd);
 }
 
 // Which operand minmod_div(dl, dr, d) returns: -1 for the constant zero, 0

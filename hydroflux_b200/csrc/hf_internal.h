@@ -4,6 +4,7 @@
 #include <cstdint>
 
 #include "../../include/hydroflux_gpu.h"
+#include "hf_arith.h"
 
 namespace hf {
 
@@ -140,6 +141,9 @@ struct StageArgs {
   int tile_base;  // first tile of this grid in an ensemble's tile list (0 alone)
   int pad_;
   double dx, dy;
+  // 1/dx and 1/dy for the divisions by the spacing (hfa::div_recip); a
+  // default (ok = false) falls back to the IEEE division.
+  hfa::RecipD rx, ry;
   const double* z;
   const double* n;
   const double* in_h;

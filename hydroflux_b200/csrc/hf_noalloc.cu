@@ -140,6 +140,8 @@ extern "C" int hf_ssprk2_step_noalloc(const hf_grid* grid, double* h, double* hu
   a.tiles_y = (int)((grid->n_rows + TY - 1) / TY);
   a.dx = grid->dx;
   a.dy = grid->dy;
+  a.rx = hfa::make_recip(a.dx);
+  a.ry = hfa::make_recip(a.dy);
   a.z = grid->bed;
   a.n = grid->manning;
   for (int k = 0; k < 4; ++k) {

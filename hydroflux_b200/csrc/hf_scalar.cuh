@@ -70,6 +70,15 @@ __device__ __forceinline__ DualD dvp(double a, DualD b) {
   return DualD{hfa::div_rn_pos(a, b.v), hfa::div_rn(-a * b.d, b.v * b.v)};
 }
 
+// Division by a grid spacing through its precomputed reciprocal (the same
+// correctly rounded quotient as dvp; hfa::div_recip).
+__device__ __forceinline__ double dvr(double a, const hfa::RecipD& r) {
+  return hfa::div_recip(a, r);
+}
+__device__ __forceinline__ DualD dvr(DualD a, const hfa::RecipD& r) {
+  return DualD{hfa::div_recip(a.v, r), hfa::div_recip(a.d, r)};
+}
+
 // sqrt (dual.rs:46-50): derivative 0 where the root is 0.
 __device__ __forceinline__ double r_sqrt(double x) { return hfa::sqrt_rn(x); }
 __device__ __forceinline__ DualD r_sqrt(DualD x) {

@@ -315,6 +315,8 @@ int hf_server_admit(hf_server* v, const hf_scenario_desc* d, int* slot_out) {
   x.tiles_y = s.tiles_y;
   x.dx = d->mesh.dx;
   x.dy = d->mesh.dy;
+  x.rx = hfa::make_recip(x.dx);
+  x.ry = hfa::make_recip(x.dy);
   x.z = z;
   x.n = nm;
   x.bc = boundaries_dev(d->cfg.boundaries);

@@ -268,7 +268,7 @@ __device__ __forceinline__ void stage_tile_faces(const StageArgs& A, StageSmemT<
       const int na = xd ? nc : nr;
       const int st4 = xd ? 1 : R4W;
       const int st3 = xd ? 1 : R3W;
-      const double d = xd ? dx : dy;
+      const hfa::RecipD& rd = xd ? A.rx : A.ry;
       T se = Z, su = Z, sv = Z;
       if (na >= 2) {
         const int lo = max(ga - 2, 0) - ga, hi = min(ga + 2, na - 1) - ga;
@@ -279,19 +279,19 @@ __device__ __forceinline__ void stage_tile_faces(const StageArgs& A, StageSmemT<
           const int c3 = i3(li, lj);
           if (ga == 0) {
             const int r3 = c3 + st3;
-            se = dvp(S.eta[r3] - S.eta[c3], d);  // d = dx or dy > 0
-            su = dvp(S.u[r3] - S.u[c3], d);
-            sv = dvp(S.v[r3] - S.v[c3], d);
+            se = dvr(S.eta[r3] - S.eta[c3], rd);  // / dx or / dy
+            su = dvr(S.u[r3] - S.u[c3], rd);
+            sv = dvr(S.v[r3] - S.v[c3], rd);
           } else if (ga == na - 1) {
             const int l3 = c3 - st3;
-            se = dvp(S.eta[c3] - S.eta[l3], d);
-            su = dvp(S.u[c3] - S.u[l3], d);
-            sv = dvp(S.v[c3] - S.v[l3], d);
+            se = dvr(S.eta[c3] - S.eta[l3], rd);
+            su = dvr(S.u[c3] - S.u[l3], rd);
+            sv = dvr(S.v[c3] - S.v[l3], rd);
           } else {
             const int l3 = c3 - st3, r3 = c3 + st3;
-            se = minmod_div<T>(S.eta[c3] - S.eta[l3], S.eta[r3] - S.eta[c3], d);
-            su = minmod_div<T>(S.u[c3] - S.u[l3], S.u[r3] - S.u[c3], d);
-            sv = minmod_div<T>(S.v[c3] - S.v[l3], S.v[r3] - S.v[c3], d);
+            se = minmod_div<T>(S.eta[c3] - S.eta[l3], S.eta[r3] - S.eta[c3], rd);
+            su = minmod_div<T>(S.u[c3] - S.u[l3], S.u[r3] - S.u[c3], rd);
+            sv = minmod_div<T>(S.v[c3] - S.v[l3], S.v[r3] - S.v[c3], rd);
           }
         }
       }
@@ -521,13 +521,13 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, StageSmemT<T>& S,
         const T eta_right = gj + 1 < nc ? eta_cell + sex * (0.5 * dx) : eta_cell;
         const T hfl = r_max(eta_left - zfl, Z);
         const T hfr = r_max(eta_right - zfr, Z);
-        const T s_hu = dvp((hfl + hfr) * ((eta_left - hfl) - (eta_right - hfr)) * (0.5 * GRAVITY), dx);
+        const T s_hu = dvr((hfl + hfr) * ((eta_left - hfl) - (eta_right - hfr)) * (0.5 * GRAVITY), A.rx);
         const T sey = S.sye[isy(li, lj)];
         const T eta_top = gi > 0 ? eta_cell - sey * (0.5 * dy) : eta_cell;
         const T eta_bot = gi + 1 < nr ? eta_cell + sey * (0.5 * dy) : eta_cell;
         const T hft = r_max(eta_top - zft, Z);
         const T hfb = r_max(eta_bot - zfb, Z);
-        const T s_hv = dvp((hft + hfb) * ((eta_top - hft) - (eta_bot - hfb)) * (0.5 * GRAVITY), dy);
+        const T s_hv = dvr((hft + hfb) * ((eta_top - hft) - (eta_bot - hfb)) * (0.5 * GRAVITY), A.ry);
 
         if (val(new_h) <= H_VEL) {
           nh = r_max(new_h, Z);  // moisture floor keeps the mass
