@@ -51,6 +51,24 @@ __device__ void lane_args(const StageArgs& A, int lane, StageArgs& L) {
   L.out_h = L.out_hu = L.out_hv = nullptr;
 }
 
+// A tile whose 4-cell halo lies inside the grid reaches no side: it runs the
+// stage with the boundary branches compiled out (same arithmetic).
+__device__ __forceinline__ bool interior_tile(const StageArgs& A, int tile) {
+  const int tyi = tile / A.tiles_x;
+  const int gi0 = tyi * TY, gj0 = (tile - tyi * A.tiles_x) * TX;
+  return gi0 >= 4 && gj0 >= 4 && gi0 + TY + 4 <= A.nr && gj0 + TX + 4 <= A.nc;
+}
+
+template <class T>
+__device__ __forceinline__ void stage_tile_any(const StageArgs& A, StageSmemT<T>& S, int tile,
+                                               double& sxm, double& sym,
+                                               unsigned long long& nonfin) {
+  if (interior_tile(A, tile))
+    stage_tile<T, false, true>(A, S, tile, sxm, sym, nonfin);
+  else
+    stage_tile<T>(A, S, tile, sxm, sym, nonfin);
+}
+
 // One stage of one grid over a persistent tile loop. For T = DualD,
 // blockIdx.y is the tangent lane (vector mode); the CFL reduction and the
 // clock belong to lane 0.
@@ -68,10 +86,10 @@ __global__ void __launch_bounds__(NTHREADS, StageOcc<T>::value) k_stage(const St
     if (threadIdx.x == 0) lane_args(A, blockIdx.y, L);
     __syncthreads();
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
-      stage_tile<T>(L, S, tile, sxm, sym, nonfin);
+      stage_tile_any<T>(L, S, tile, sxm, sym, nonfin);
   } else {
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
-      stage_tile<T>(A, S, tile, sxm, sym, nonfin);
+      stage_tile_any<T>(A, S, tile, sxm, sym, nonfin);
   }
   if (A.finalize && blockIdx.y == 0) {
     block_reduce_speeds(sxm, sym, nonfin, A.ctrl);
@@ -95,7 +113,10 @@ __global__ void __launch_bounds__(NTHREADS, HF_MIN_BLOCKS) k_stage_pf(const Stag
     cp_async_wait_all();
     __syncthreads();
     const int next = tile + (int)gridDim.x < ntiles ? tile + (int)gridDim.x : -1;
-    stage_tile<double, true>(A, P.s, tile, sxm, sym, nonfin, P.hst, next);
+    if (interior_tile(A, tile))
+      stage_tile<double, true, true>(A, P.s, tile, sxm, sym, nonfin, P.hst, next);
+    else
+      stage_tile<double, true>(A, P.s, tile, sxm, sym, nonfin, P.hst, next);
   }
   if (A.finalize) {
     block_reduce_speeds(sxm, sym, nonfin, A.ctrl);
@@ -125,7 +146,7 @@ __device__ __forceinline__ void batch_tile(const StageArgs* __restrict__ args,
   if (!A.ctrl->active) return;  // uniform over the CTA
   double sxm = 0.0, sym = 0.0;
   unsigned long long nonfin = 0;
-  stage_tile<double>(A, S, tile_local ? tile_local[t] : t - A.tile_base, sxm, sym, nonfin);
+  stage_tile_any<double>(A, S, tile_local ? tile_local[t] : t - A.tile_base, sxm, sym, nonfin);
   if (A.finalize) block_reduce_speeds(sxm, sym, nonfin, A.ctrl);
 }
 

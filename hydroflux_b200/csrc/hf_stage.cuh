@@ -109,9 +109,12 @@ __device__ __forceinline__ void finalize_cell(const StageArgs& A, const Ctrl* c,
 
 // CFL contribution of one cell of the final state, with the ghost cells of
 // the sides it touches (cfl_time_step_with_bcs, update.rs:170-208).
+// IN: the cell is known not to touch a side (an interior tile).
+template <bool IN = false>
 __device__ __forceinline__ void cfl_cell(const StageArgs& A, int gi, int gj, int64_t g, double h,
                                          double hu, double hv, double& sx, double& sy) {
   cell_speeds(h, hu, hv, sx, sy);
+  if constexpr (IN) return;
   const int nr = A.nr, nc = A.nc;
   const double* dn = nullptr;
   if (gj == 0)
@@ -186,7 +189,7 @@ __device__ __forceinline__ void stage_prefetch(const StageArgs& A, StageSmem& S,
 // (stage_prefetch into hst, S.eta, S.u, S.v, completed by the caller), and
 // once the faces are done the copies of tile `next` (if >= 0) are started,
 // overlapping the alpha and update phases of this tile.
-template <class T, bool PF = false>
+template <class T, bool PF = false, bool IN = false>
 __device__ __forceinline__ void stage_tile_faces(const StageArgs& A, StageSmemT<T>& S, int gi0,
                                                  int gj0, double dt, double* hst = nullptr,
                                                  int next = -1) {
@@ -224,7 +227,7 @@ __device__ __forceinline__ void stage_tile_faces(const StageArgs& A, StageSmemT<
     for (int k = tid; k < R4N; k += NTHREADS) {
       const int r = k / R4W, cc = k - r * R4W;
       const int gi = gi0 + r - 4, gj = gj0 + cc - 4;
-      const bool real = gi >= 0 && gi < nr && gj >= 0 && gj < nc;
+      const bool real = IN || (gi >= 0 && gi < nr && gj >= 0 && gj < nc);
       const int64_t g = (int64_t)gi * nc + gj;
       const T hh = real ? Field<T>::ld(A.in_h, A.tan.in_h, g) : Z;
       S.h[k] = hh;
@@ -263,26 +266,26 @@ __device__ __forceinline__ void stage_tile_faces(const StageArgs& A, StageSmemT<
         lj = kk - r * SYW - 1;
       }
       const int gi = gi0 + li, gj = gj0 + lj;
-      if (gi < 0 || gi >= nr || gj < 0 || gj >= nc) continue;
+      if (!IN && (gi < 0 || gi >= nr || gj < 0 || gj >= nc)) continue;
       const int ga = xd ? gj : gi;
       const int na = xd ? nc : nr;
       const int st4 = xd ? 1 : R4W;
       const int st3 = xd ? 1 : R3W;
       const hfa::RecipD& rd = xd ? A.rx : A.ry;
       T se = Z, su = Z, sv = Z;
-      if (na >= 2) {
-        const int lo = max(ga - 2, 0) - ga, hi = min(ga + 2, na - 1) - ga;
+      if (IN || na >= 2) {
+        const int lo = IN ? -2 : max(ga - 2, 0) - ga, hi = IN ? 2 : min(ga + 2, na - 1) - ga;
         const int c4 = i4(li, lj);
         bool anyd = false;
         for (int o = lo; o <= hi; ++o) anyd |= val(S.h[c4 + o * st4]) <= H_DRY;
         if (!anyd) {
           const int c3 = i3(li, lj);
-          if (ga == 0) {
+          if (!IN && ga == 0) {
             const int r3 = c3 + st3;
             se = dvr(S.eta[r3] - S.eta[c3], rd);  // / dx or / dy
             su = dvr(S.u[r3] - S.u[c3], rd);
             sv = dvr(S.v[r3] - S.v[c3], rd);
-          } else if (ga == na - 1) {
+          } else if (!IN && ga == na - 1) {
             const int l3 = c3 - st3;
             se = dvr(S.eta[c3] - S.eta[l3], rd);
             su = dvr(S.u[c3] - S.u[l3], rd);
@@ -324,11 +327,11 @@ __device__ __forceinline__ void stage_tile_faces(const StageArgs& A, StageSmemT<
       const int na = xd ? nc : nr;
       const int gx = xd ? gi0 + li : gj0 + lj;  // index across
       const int nx = xd ? nr : nc;
-      if (gx < 0 || gx >= nx || gf < 0 || gf > na) continue;
+      if (!IN && (gx < 0 || gx >= nx || gf < 0 || gf > na)) continue;
       const int mi = xd ? li : li - 1, mj = xd ? lj - 1 : lj;  // minus (left/top) cell
       const int pi = li, pj = lj;                               // plus (right/bottom) cell
       T m, nmn, npl, tg;
-      if (gf == 0 || gf == na) {
+      if (!IN && (gf == 0 || gf == na)) {
         const bool lo_side = gf == 0;
         const int ci = lo_side ? pi : mi, cj = lo_side ? pj : mj;
         const int64_t g0 = (int64_t)(gi0 + ci) * nc + (gj0 + cj);
@@ -408,7 +411,7 @@ __device__ __forceinline__ void stage_tile_faces(const StageArgs& A, StageSmemT<
       const int li = r - 1, lj = k - r * AW - 1;
       if ((li < 0 || li >= TY) && (lj < 0 || lj >= TX)) continue;
       const int gi = gi0 + li, gj = gj0 + lj;
-      if (gi < 0 || gi >= nr || gj < 0 || gj >= nc) continue;
+      if (!IN && (gi < 0 || gi >= nr || gj < 0 || gj >= nc)) continue;
       const T fr = S.fxm[ifx(li, lj + 1)], fl = S.fxm[ifx(li, lj)];
       const T fb = S.fym[ify(li + 1, lj)], ft = S.fym[ify(li, lj)];
       T out = Z;
@@ -424,24 +427,25 @@ __device__ __forceinline__ void stage_tile_faces(const StageArgs& A, StageSmemT<
 }
 
 // Face beds of a tile cell's four faces (update.rs:676-728, 650-656).
+template <bool IN = false>
 __device__ __forceinline__ void cell_face_beds(const StageArgs& A, const double* Sz, bool dc,
                                                bool dl, bool dr, bool dt_, bool db, int c3,
                                                int gi, int gj, double& zfl, double& zfr,
                                                double& zft, double& zfb) {
   const double zc = Sz[c3];
-  if (gj == 0)
+  if (!IN && gj == 0)
     zfl = (ghost_bed(A.bc.kind[SIDE_WEST], zc, Sz[c3 + 1]) + zc) * 0.5;
   else
     zfl = (dl != dc) ? fmax(Sz[c3 - 1], zc) : (Sz[c3 - 1] + zc) * 0.5;
-  if (gj + 1 == A.nc)
+  if (!IN && gj + 1 == A.nc)
     zfr = (zc + ghost_bed(A.bc.kind[SIDE_EAST], zc, Sz[c3 - 1])) * 0.5;
   else
     zfr = (dc != dr) ? fmax(zc, Sz[c3 + 1]) : (zc + Sz[c3 + 1]) * 0.5;
-  if (gi == 0)
+  if (!IN && gi == 0)
     zft = (ghost_bed(A.bc.kind[SIDE_NORTH], zc, Sz[c3 + R3W]) + zc) * 0.5;
   else
     zft = (dt_ != dc) ? fmax(Sz[c3 - R3W], zc) : (Sz[c3 - R3W] + zc) * 0.5;
-  if (gi + 1 == A.nr)
+  if (!IN && gi + 1 == A.nr)
     zfb = (zc + ghost_bed(A.bc.kind[SIDE_SOUTH], zc, Sz[c3 - R3W])) * 0.5;
   else
     zfb = (dc != db) ? fmax(zc, Sz[c3 + R3W]) : (zc + Sz[c3 + R3W]) * 0.5;
@@ -450,7 +454,9 @@ __device__ __forceinline__ void cell_face_beds(const StageArgs& A, const double*
 // One forward-Euler stage (update.rs:805-1211) on one tile of one grid. Called
 // by every thread of the CTA; accumulates the CTA's CFL maxima for the
 // finalize epilogue into (sxm, sym, nonfin).
-template <class T, bool PF = false>
+// IN: the tile and its 4-cell halo lie inside the grid (no side is reached),
+// so the boundary branches compile away; the arithmetic is the same.
+template <class T, bool PF = false, bool IN = false>
 __device__ __forceinline__ void stage_tile(const StageArgs& A, StageSmemT<T>& S, int tile,
                                            double& sxm, double& sym, unsigned long long& nonfin,
                                            double* hst = nullptr, int next = -1) {
@@ -465,7 +471,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, StageSmemT<T>& S,
   {
     const int tyi = tile / A.tiles_x;
     const int gi0 = tyi * TY, gj0 = (tile - tyi * A.tiles_x) * TX;
-    stage_tile_faces<T, PF>(A, S, gi0, gj0, dt, hst, next);
+    stage_tile_faces<T, PF, IN>(A, S, gi0, gj0, dt, hst, next);
 
     // ---- FV update + bed source + floor: update.rs:1071-1210
     int src_lo = 0, src_hi = 0;
@@ -477,13 +483,13 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, StageSmemT<T>& S,
     for (int q = 0; q < CELLS_PER_THREAD; ++q) {
       const int li = tid / TX + ROWS_PER_PASS * q, lj = tid % TX;
       const int gi = gi0 + li, gj = gj0 + lj;
-      if (gi >= nr || gj >= nc) continue;
+      if (!IN && (gi >= nr || gj >= nc)) continue;
       const int64_t g = (int64_t)gi * nc + gj;
       const int c4 = i4(li, lj), c3 = i3(li, lj);
       const T hc = S.h[c4];
       const bool dc = val(hc) <= H_DRY;
       T nh, nhu, nhv;
-      if (dc && gi > 0 && gi + 1 < nr && gj > 0 && gj + 1 < nc && val(S.h[c4 - R4W]) <= H_DRY &&
+      if (dc && (IN || (gi > 0 && gi + 1 < nr && gj > 0 && gj + 1 < nc)) && val(S.h[c4 - R4W]) <= H_DRY &&
           val(S.h[c4 + R4W]) <= H_DRY && val(S.h[c4 - 1]) <= H_DRY && val(S.h[c4 + 1]) <= H_DRY) {
         nh = hc;  // isolated-dry fast path (update.rs:1072-1088)
         nhu = Z;
@@ -495,10 +501,10 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, StageSmemT<T>& S,
         const T one = cst<T>(1.0);
         // Upstream alpha per face (update.rs:992-1053). Dry-dry interior faces
         // are exact zeros; scaling them by an alpha in [0, 1] keeps them +0.
-        const T ar = (gj + 1 == nc) ? (val(mr) > 0.0 ? ac : one) : (val(mr) > 0.0 ? ac : S.a[ia(li, lj + 1)]);
-        const T al = (gj == 0) ? (val(ml) < 0.0 ? ac : one) : (val(ml) > 0.0 ? S.a[ia(li, lj - 1)] : ac);
-        const T ab = (gi + 1 == nr) ? (val(mb) > 0.0 ? ac : one) : (val(mb) > 0.0 ? ac : S.a[ia(li + 1, lj)]);
-        const T at = (gi == 0) ? (val(mt) < 0.0 ? ac : one) : (val(mt) > 0.0 ? S.a[ia(li - 1, lj)] : ac);
+        const T ar = (!IN && gj + 1 == nc) ? (val(mr) > 0.0 ? ac : one) : (val(mr) > 0.0 ? ac : S.a[ia(li, lj + 1)]);
+        const T al = (!IN && gj == 0) ? (val(ml) < 0.0 ? ac : one) : (val(ml) > 0.0 ? S.a[ia(li, lj - 1)] : ac);
+        const T ab = (!IN && gi + 1 == nr) ? (val(mb) > 0.0 ? ac : one) : (val(mb) > 0.0 ? ac : S.a[ia(li + 1, lj)]);
+        const T at = (!IN && gi == 0) ? (val(mt) < 0.0 ? ac : one) : (val(mt) > 0.0 ? S.a[ia(li - 1, lj)] : ac);
         const T fxr_m = mr * ar, fxr_n = S.fxnm[fr] * ar, fxr_t = S.fxt[fr] * ar;
         const T fxl_m = ml * al, fxl_n = S.fxnp[fl] * al, fxl_t = S.fxt[fl] * al;
         const T fyb_m = mb * ab, fyb_n = S.fynm[fb] * ab, fyb_t = S.fyt[fb] * ab;
@@ -509,7 +515,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, StageSmemT<T>& S,
         const T dhv = (fxr_t - fxl_t) * dt_dx + (fyb_n - fyt_n) * dt_dy;
 
         double zfl, zfr, zft, zfb;
-        cell_face_beds(A, S.z, dc, val(S.h[c4 - 1]) <= H_DRY, val(S.h[c4 + 1]) <= H_DRY,
+        cell_face_beds<IN>(A, S.z, dc, val(S.h[c4 - 1]) <= H_DRY, val(S.h[c4 + 1]) <= H_DRY,
                        val(S.h[c4 - R4W]) <= H_DRY, val(S.h[c4 + R4W]) <= H_DRY, c3, gi, gj, zfl,
                        zfr, zft, zfb);
 
@@ -517,14 +523,14 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, StageSmemT<T>& S,
         const double zc = S.z[c3];
         const T eta_cell = hc + zc;
         const T sex = S.sxe[isx(li, lj)];
-        const T eta_left = gj > 0 ? eta_cell - sex * (0.5 * dx) : eta_cell;
-        const T eta_right = gj + 1 < nc ? eta_cell + sex * (0.5 * dx) : eta_cell;
+        const T eta_left = (IN || gj > 0) ? eta_cell - sex * (0.5 * dx) : eta_cell;
+        const T eta_right = (IN || gj + 1 < nc) ? eta_cell + sex * (0.5 * dx) : eta_cell;
         const T hfl = r_max(eta_left - zfl, Z);
         const T hfr = r_max(eta_right - zfr, Z);
         const T s_hu = dvr((hfl + hfr) * ((eta_left - hfl) - (eta_right - hfr)) * (0.5 * GRAVITY), A.rx);
         const T sey = S.sye[isy(li, lj)];
-        const T eta_top = gi > 0 ? eta_cell - sey * (0.5 * dy) : eta_cell;
-        const T eta_bot = gi + 1 < nr ? eta_cell + sey * (0.5 * dy) : eta_cell;
+        const T eta_top = (IN || gi > 0) ? eta_cell - sey * (0.5 * dy) : eta_cell;
+        const T eta_bot = (IN || gi + 1 < nr) ? eta_cell + sey * (0.5 * dy) : eta_cell;
         const T hft = r_max(eta_top - zft, Z);
         const T hfb = r_max(eta_bot - zfb, Z);
         const T s_hv = dvr((hft + hfb) * ((eta_top - hft) - (eta_bot - hfb)) * (0.5 * GRAVITY), A.ry);
@@ -559,7 +565,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, StageSmemT<T>& S,
       }
       if (A.finalize) {
         finalize_cell<T>(A, ctrl, dt, gi, gj, g, src_lo, src_hi, nh, nhu, nhv);
-        cfl_cell(A, gi, gj, g, val(nh), val(nhu), val(nhv), sxm, sym);
+        cfl_cell<IN>(A, gi, gj, g, val(nh), val(nhu), val(nhv), sxm, sym);
         if (ctrl->check_finite && !isfinite(val(nh))) ++nonfin;
       }
       Field<T>::st(A.out_h, A.tan.out_h, g, nh);
