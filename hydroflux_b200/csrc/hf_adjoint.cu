@@ -116,7 +116,10 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_stage_adj(const StageArgs A, co
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int tyi = tile / A.tiles_x;
     const int gi0 = tyi * TY, gj0 = (tile - tyi * A.tiles_x) * TX;
-    stage_tile_faces<double>(A, S, gi0, gj0, dt);
+    if (interior_tile(A, tile))
+      stage_tile_faces<double, false, true>(A, S, gi0, gj0, dt);
+    else
+      stage_tile_faces<double>(A, S, gi0, gj0, dt);
 
     // ---- A: per tile cell, epilogue / combination / update in reverse
     int src_lo = 0, src_hi = 0;

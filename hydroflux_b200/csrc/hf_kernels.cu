@@ -51,14 +51,6 @@ __device__ void lane_args(const StageArgs& A, int lane, StageArgs& L) {
   L.out_h = L.out_hu = L.out_hv = nullptr;
 }
 
-// A tile whose 4-cell halo lies inside the grid reaches no side: it runs the
-// stage with the boundary branches compiled out (same arithmetic).
-__device__ __forceinline__ bool interior_tile(const StageArgs& A, int tile) {
-  const int tyi = tile / A.tiles_x;
-  const int gi0 = tyi * TY, gj0 = (tile - tyi * A.tiles_x) * TX;
-  return gi0 >= 4 && gj0 >= 4 && gi0 + TY + 4 <= A.nr && gj0 + TX + 4 <= A.nc;
-}
-
 template <class T>
 __device__ __forceinline__ void stage_tile_any(const StageArgs& A, StageSmemT<T>& S, int tile,
                                                double& sxm, double& sym,
