@@ -94,10 +94,21 @@ def problem(workloads, name):
               bcs=((1, 0.0), (1, 0.0), (2, 0.6), (3, 0.05)), cfl=0.45, t_end=1e9, max_dt=0.5,
               sources=[(10, 20, np.array([0.0, 10.0, 40.0]), np.array([0.0, 2.0, 0.5]))])
         return s, 150, np.array([10 * nc + 3, 5 * nc + 12, 14 * nc + 30])
+    if name == "wide":  # SSP-RK2 dam break whose front crosses interior tiles
+        nr, nc = 40, 84
+        x = np.arange(nc)[None, :] + 0.0 * np.arange(nr)[:, None]
+        h = np.where(x < 40, 1.2, 0.0)
+        z = 0.01 * x + 0.04 * np.sin(0.5 * np.arange(nr))[:, None]
+        s = S("wide", z, lognormal(rng, (nr, nc)), 1.0, 1.0, h, np.zeros_like(h),
+              np.zeros_like(h), bcs=((1, 0.0), (0, 0.0), (1, 0.0), (0, 0.0)), cfl=0.45,
+              t_end=1e9, max_dt=1.0, rain=(np.array([0.0]), np.array([1e-4])))
+        return s, 80, np.array([12 * nc + 36, 20 * nc + 44, 30 * nc + 50, 16 * nc + 60])
     raise KeyError(name)
 
 
-PROBLEMS = ["valley", "dambreak_fe", "inflow"]
+# "wide" (40 x 84) has interior tiles, whose boundary branches are compiled
+# out; the other grids are all edge tiles.
+PROBLEMS = ["valley", "dambreak_fe", "inflow", "wide"]
 
 
 def observations(cal, s, n_steps, G, seed):

@@ -56,8 +56,11 @@ def random_case(nr, nc, seed, wet=0.7, film=0.05, slope=0.02):
     return z, n, h, hu, hv
 
 
+# 20x68 has exactly one tile whose 4-cell halo just fits inside the grid (the
+# interior-tile instantiation at its threshold on all four sides); 20x67 has
+# none; 40x70 and 64x96 mix both kinds.
 SHAPES = [(1, 1), (1, 9), (9, 1), (2, 2), (3, 3), (5, 7), (16, 32), (17, 33), (33, 17),
-          (40, 70), (64, 96)]
+          (20, 67), (20, 68), (40, 70), (64, 96)]
 BC_SETS = {
     "walls": ((1, 0),) * 4,
     "trans": ((0, 0),) * 4,
