@@ -1,7 +1,8 @@
-"""The Rust shim written out in INTEGRATION.md against include/hydroflux_gpu.h.
+"""The Rust shim of the integration guide against include/hydroflux_gpu.h.
 
-There is no Rust toolchain here, so the shim a maintainer would paste into
-the crate is not compiled. This test stands in for the compile-time half of
+The guide writes out, in its ```rust blocks, the FFI declarations a
+maintainer would paste into the crate. There is no Rust toolchain here, so
+that shim is not compiled. This test stands in for the compile-time half of
 that: every `extern "C"` function of the shim must exist in the header with
 the same return and parameter types, and every `#[repr(C)]` struct must list
 the header struct's fields in the same order with the same types."""
