@@ -26,9 +26,9 @@
 namespace hf {
 
 // Blocks per SM the stage kernel is compiled for: the f64 tile takes 66 KB
-// of shared memory (three CTAs per SM), the DualD tile 129 KB (one).
+// of shared memory (three CTAs per SM), the DualD tile 112 KB (two).
 template <class T> struct StageOcc { static constexpr int value = HF_MIN_BLOCKS; };
-template <> struct StageOcc<DualD> { static constexpr int value = 1; };
+template <> struct StageOcc<DualD> { static constexpr int value = 2; };
 
 // The arguments of tangent lane `lane`: its tangent arrays, and no value
 // outputs unless it is lane 0 (the values are the same in every lane).
@@ -555,6 +555,9 @@ int stage_dual_grid_size(int tiles, int device) {
     DevGuard dg(device);
     cudaFuncSetAttribute(k_stage<DualD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)sizeof(StageSmemT<DualD>));
+    // two 112 KB tiles per SM need the largest shared-memory carveout
+    cudaFuncSetAttribute(k_stage<DualD>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         (int)cudaSharedmemCarveoutMaxShared);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stage<DualD>, NTHREADS,
                                                   sizeof(StageSmemT<DualD>));
     if (per_sm < 1) per_sm = 1;

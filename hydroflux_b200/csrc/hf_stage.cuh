@@ -35,6 +35,27 @@ template <class T> struct StageSmemT {
 };
 using StageSmem = StageSmemT<double>;
 
+// The DualD tile would take 129 KB in the layout above: one CTA per SM. It
+// runs the slopes and faces as an x pass and then a y pass (SplitFaces), so
+// the x momentum slopes are dead before the y ones are written and both
+// share storage, as does alpha once the y faces are done: 112 KB, two CTAs
+// per SM. The eta slopes of both directions stay (the bed source reads them).
+template <> struct StageSmemT<DualD> {
+  DualD h[R4N];
+  double z[R3N];
+  DualD eta[R3N], u[R3N], v[R3N];
+  DualD sxe[SXN], sye[SYN];
+  DualD fxm[FXN], fxnm[FXN], fxnp[FXN], fxt[FXN];
+  DualD fym[FYN], fynm[FYN], fynp[FYN], fyt[FYN];
+  union {
+    struct { DualD sxu[SXN], sxv[SXN]; };
+    struct { DualD syu[SYN], syv[SYN]; };
+    DualD a[AN];
+  };
+};
+template <class T> struct SplitFaces { static constexpr bool value = false; };
+template <> struct SplitFaces<DualD> { static constexpr bool value = true; };
+
 __device__ __forceinline__ int i4(int li, int lj) { return (li + 4) * R4W + (lj + 4); }
 __device__ __forceinline__ int i3(int li, int lj) { return (li + 3) * R3W + (lj + 3); }
 __device__ __forceinline__ int isx(int li, int lj) { return (li + 1) * SXW + (lj + 2); }
@@ -252,8 +273,8 @@ __device__ __forceinline__ void stage_tile_faces(const StageArgs& A, StageSmemT<
     __syncthreads();
   }
   {
-    // ---- limited slopes: update.rs:459-540
-    for (int k = tid; k < SXN + SYN; k += NTHREADS) {
+    // ---- limited slopes: update.rs:459-540 (item k < SXN: x slope, else y)
+    auto slope_item = [&](int k) {
       const bool xd = k < SXN;
       int li, lj;
       if (xd) {
@@ -266,7 +287,7 @@ __device__ __forceinline__ void stage_tile_faces(const StageArgs& A, StageSmemT<
         lj = kk - r * SYW - 1;
       }
       const int gi = gi0 + li, gj = gj0 + lj;
-      if (!IN && (gi < 0 || gi >= nr || gj < 0 || gj >= nc)) continue;
+      if (!IN && (gi < 0 || gi >= nr || gj < 0 || gj >= nc)) return;
       const int ga = xd ? gj : gi;
       const int na = xd ? nc : nr;
       const int st4 = xd ? 1 : R4W;
@@ -307,11 +328,10 @@ __device__ __forceinline__ void stage_tile_faces(const StageArgs& A, StageSmemT<
         S.syu[k - SXN] = su;
         S.syv[k - SXN] = sv;
       }
-    }
-    __syncthreads();
+    };
 
-    // ---- faces: update.rs:676-728 (face beds), 890-926 (fluxes)
-    for (int k = tid; k < FXN + FYN; k += NTHREADS) {
+    // ---- faces: update.rs:676-728 (face beds), 890-926 (fluxes) (item k < FXN: x face)
+    auto face_item = [&](int k) {
       const bool xd = k < FXN;
       int li, lj;  // x face: (row li, face lj); y face: (face li, column lj)
       if (xd) {
@@ -327,7 +347,7 @@ __device__ __forceinline__ void stage_tile_faces(const StageArgs& A, StageSmemT<
       const int na = xd ? nc : nr;
       const int gx = xd ? gi0 + li : gj0 + lj;  // index across
       const int nx = xd ? nr : nc;
-      if (!IN && (gx < 0 || gx >= nx || gf < 0 || gf > na)) continue;
+      if (!IN && (gx < 0 || gx >= nx || gf < 0 || gf > na)) return;
       const int mi = xd ? li : li - 1, mj = xd ? lj - 1 : lj;  // minus (left/top) cell
       const int pi = li, pj = lj;                               // plus (right/bottom) cell
       T m, nmn, npl, tg;
@@ -399,8 +419,23 @@ __device__ __forceinline__ void stage_tile_faces(const StageArgs& A, StageSmemT<
         const int kk = k - FXN;
         S.fym[kk] = m; S.fynm[kk] = nmn; S.fynp[kk] = npl; S.fyt[kk] = tg;
       }
+    };
+
+    if constexpr (!SplitFaces<T>::value) {
+      for (int k = tid; k < SXN + SYN; k += NTHREADS) slope_item(k);
+      __syncthreads();
+      for (int k = tid; k < FXN + FYN; k += NTHREADS) face_item(k);
+      __syncthreads();
+    } else {  // x slopes, x faces, then y slopes (over the x momentum slopes), y faces
+      for (int k = tid; k < SXN; k += NTHREADS) slope_item(k);
+      __syncthreads();
+      for (int k = tid; k < FXN; k += NTHREADS) face_item(k);
+      __syncthreads();
+      for (int k = SXN + tid; k < SXN + SYN; k += NTHREADS) slope_item(k);
+      __syncthreads();
+      for (int k = FXN + tid; k < FXN + FYN; k += NTHREADS) face_item(k);
+      __syncthreads();
     }
-    __syncthreads();
     if constexpr (PF) {
       if (next >= 0) stage_prefetch(A, S, hst, next);  // eta, u, v and hst are dead now
     }
