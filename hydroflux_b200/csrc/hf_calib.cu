@@ -131,6 +131,11 @@ struct hf_calib {
   double* Ualt[3] = {nullptr, nullptr, nullptr};  // second value buffer (no in-place stage 2)
   // forward runs replayed from CUDA graphs: [mode][checkpoints][1 / 8 / 64 steps]
   cudaGraphExec_t fgraphs[3][2][3] = {};
+  // vector-mode runs replayed from CUDA graphs of 2 / 8 / 64 steps, captured
+  // for `lgraph_lanes` lanes. Every chunk is an even number of steps, so it
+  // starts and ends with the values in U (the steps alternate U and Ualt).
+  cudaGraphExec_t lgraphs[3] = {};
+  int lgraph_lanes = 0;
 };
 
 namespace {
@@ -230,6 +235,7 @@ int status_of_run(hf_calib* c, int64_t* n_run) {
 // initial tangent; CFL dt from values, recorded). With checkpoints the state
 // before every C-th step is stored.
 const int kFwdChunk[3] = {1, 8, 64};
+const int kLaneChunk[3] = {2, 8, 64};
 
 // The launches of one forward step (see forward_run).
 int enqueue_forward_step(hf_calib* c, int mode, bool checkpoints, const StageArgs& a1,
@@ -501,6 +507,8 @@ void destroy_calib(hf_calib* c) {
     for (auto& k : m)
       for (auto& g : k)
         if (g) cudaGraphExecDestroy(g);
+  for (auto& g : c->lgraphs)
+    if (g) cudaGraphExecDestroy(g);
   c->forcing.release_rain();
   c->forcing.release_src();
   std::vector<void*> ptrs = {c->z,    c->n,    c->dn,   c->h0,   c->hu0,  c->hv0,  c->cells,
@@ -537,7 +545,17 @@ int upload_tangent_init(hf_calib* c, const double* dh0, const double* dhu0, cons
   return HF_OK;
 }
 
+void drop_lane_graphs(hf_calib* c) {
+  for (auto& g : c->lgraphs)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+  c->lgraph_lanes = 0;
+}
+
 void free_lanes(hf_calib* c) {
+  drop_lane_graphs(c);  // they hold the lane buffers' addresses
   for (int f = 0; f < 3; ++f) {
     for (double** p : {&c->dUL[f], &c->dU1L[f]})
       if (*p) {
@@ -586,13 +604,14 @@ int forward_run_lanes(hf_calib* c, int lanes, int64_t* n_run) {
   // partial wave would double the stage time).
   const int cap = stage_dual_grid_size(1 << 30, c->device);
   const int grid = std::max(1, std::min(c->ntiles, cap / lanes));
-  double* cur[3] = {c->U[0], c->U[1], c->U[2]};
-  double* nxt[3] = {c->Ualt[0], c->Ualt[1], c->Ualt[2]};
+  double* const vU[3] = {c->U[0], c->U[1], c->U[2]};
+  double* const vA[3] = {c->Ualt[0], c->Ualt[1], c->Ualt[2]};
   {
-    StageArgs a0 = calib_args(c, cur, c->U1, nullptr, 0, 0, c->ctrl, fd);
+    StageArgs a0 = calib_args(c, vU, c->U1, nullptr, 0, 0, c->ctrl, fd);
     C_TRY(launch_cfl(a0, 1, c->grid, c->stream));
   }
-  for (int64_t k = 0; k < c->K; ++k) {
+  // One step from the values in `cur` to `nxt`.
+  auto enqueue_lane_step = [&](double* const cur[3], double* const nxt[3]) -> int {
     StageArgs a1 = calib_args(c, cur, c->U1, nullptr, 0, 0, c->ctrl, fd);
     StageArgs a2 = calib_args(c, c->U1, nxt, cur, ssp ? 1 : 0, 1, c->ctrl, fd);
     with_tangent(a1, c, c->dUL, c->dU1L, nullptr);
@@ -608,9 +627,43 @@ int forward_run_lanes(hf_calib* c, int lanes, int64_t* n_run) {
       C_TRY(launch_finalize_dual(a2, grid, c->stream, lanes));
     C_TRY(launch_calib_post(c->ctrl, nxt[0], c->dUL[0], c->cells, (int)c->G, c->gh, c->gdhL,
                             (long long)c->K, c->stream, lanes, stride));
-    // A step that did not run (the run had ended) leaves nxt unwritten.
-    for (int f = 0; f < 3; ++f) std::swap(cur[f], nxt[f]);
-    if ((k + 1) % 64 == 0 && k + 1 < c->K) {
+    return HF_OK;
+  };
+  if (c->lgraph_lanes != lanes) {
+    drop_lane_graphs(c);
+    c->lgraph_lanes = lanes;
+  }
+  // Steps that find the run ended return at once and leave the buffers as
+  // they are; the launches stop at the next chunk boundary.
+  int64_t k = 0;
+  while (k < c->K) {
+    const int64_t left = c->K - k;
+    if (left >= 2) {
+      const int which = left >= 64 ? 2 : (left >= 8 ? 1 : 0);
+      cudaGraphExec_t& ge = c->lgraphs[which];
+      if (!ge) {
+        cudaGraph_t graph = nullptr;
+        C_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        int rc = HF_OK;
+        for (int i = 0; i < kLaneChunk[which] && rc == HF_OK; ++i)
+          rc = (i % 2 == 0) ? enqueue_lane_step(vU, vA) : enqueue_lane_step(vA, vU);
+        cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+        if (rc != HF_OK) {
+          if (graph) cudaGraphDestroy(graph);
+          return rc;
+        }
+        C_CUDA(e);
+        e = cudaGraphInstantiate(&ge, graph, 0);
+        cudaGraphDestroy(graph);
+        C_CUDA(e);
+      }
+      C_CUDA(cudaGraphLaunch(ge, c->stream));
+      k += kLaneChunk[which];
+    } else {  // the last step of an odd count; k is even, so the values are in U
+      C_TRY(enqueue_lane_step(vU, vA));
+      k += 1;
+    }
+    if (k < c->K) {
       C_CUDA(cudaMemcpyAsync(c->h_ctrl, c->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost,
                              c->stream));
       C_CUDA(cudaStreamSynchronize(c->stream));

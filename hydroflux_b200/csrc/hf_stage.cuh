@@ -36,19 +36,22 @@ template <class T> struct StageSmemT {
 using StageSmem = StageSmemT<double>;
 
 // The DualD tile would take 129 KB in the layout above: one CTA per SM. It
-// runs the slopes and faces as an x pass and then a y pass (SplitFaces), so
-// the x momentum slopes are dead before the y ones are written and both
-// share storage, as does alpha once the y faces are done: 112 KB, two CTAs
-// per SM. The eta slopes of both directions stay (the bed source reads them).
+// runs the x faces before the y faces (SplitFaces), so the y faces can be
+// written over the x momentum slopes (dead once the x faces are done) and
+// alpha over the y momentum slopes (dead once the y faces are done): 112 KB,
+// two CTAs per SM. The eta slopes of both directions stay (the bed source
+// reads them).
 template <> struct StageSmemT<DualD> {
   DualD h[R4N];
   double z[R3N];
   DualD eta[R3N], u[R3N], v[R3N];
   DualD sxe[SXN], sye[SYN];
   DualD fxm[FXN], fxnm[FXN], fxnp[FXN], fxt[FXN];
-  DualD fym[FYN], fynm[FYN], fynp[FYN], fyt[FYN];
   union {
     struct { DualD sxu[SXN], sxv[SXN]; };
+    struct { DualD fym[FYN], fynm[FYN], fynp[FYN], fyt[FYN]; };
+  };
+  union {
     struct { DualD syu[SYN], syv[SYN]; };
     DualD a[AN];
   };
@@ -426,12 +429,10 @@ __device__ __forceinline__ void stage_tile_faces(const StageArgs& A, StageSmemT<
       __syncthreads();
       for (int k = tid; k < FXN + FYN; k += NTHREADS) face_item(k);
       __syncthreads();
-    } else {  // x slopes, x faces, then y slopes (over the x momentum slopes), y faces
-      for (int k = tid; k < SXN; k += NTHREADS) slope_item(k);
+    } else {  // slopes, x faces, then y faces (over the x momentum slopes)
+      for (int k = tid; k < SXN + SYN; k += NTHREADS) slope_item(k);
       __syncthreads();
       for (int k = tid; k < FXN; k += NTHREADS) face_item(k);
-      __syncthreads();
-      for (int k = SXN + tid; k < SXN + SYN; k += NTHREADS) slope_item(k);
       __syncthreads();
       for (int k = FXN + tid; k < FXN + FYN; k += NTHREADS) face_item(k);
       __syncthreads();

@@ -250,6 +250,38 @@ def test_tangent_lanes_equal_single_tangents(gpu, name):
                 assert np.array_equal(lane_states[l][k], one[k]), (l, k)
 
 
+def test_tangent_lanes_odd_steps_and_lane_counts(gpu):
+    """Vector-mode runs replay CUDA graphs of an even number of steps, finish
+    an odd count with one direct step, and keep one set of graphs per lane
+    count: 75 steps (64 + 8 + 2 + 1) with the lane count changing between
+    runs still equal the single tangents bit for bit, and the values equal
+    a plain run."""
+    calib, workloads = gpu
+    s, _, gauges = problem(workloads, "inflow")
+    K = 75
+    with calib.Calibration(s, K, gauges) as cal:
+        observations(cal, s, K, len(gauges), 11)
+        cal.run(s.manning)
+        ref = cal.final_state()
+        rng = np.random.default_rng(12)
+        ds = [directions(rng, s) for _ in range(4)]
+        singles = []
+        for d in ds:
+            dJ1 = cal.tangent(s.manning, **d)[1]
+            singles.append((dJ1, cal.final_state()))
+        for lanes in (3, 1, 4, 3):
+            stack = {k: np.stack([d[k] for d in ds[:lanes]]) for k in ds[0]}
+            _, dJ = cal.tangent_lanes(s.manning, **stack)
+            st = cal.final_state()
+            for k in ("h", "hu", "hv"):
+                assert np.array_equal(st[k], ref[k]), (lanes, k)
+            for l in range(lanes):
+                assert dJ[l] == singles[l][0], (lanes, l)
+                one = cal.lane_state(l)
+                for k in ("dh", "dhu", "dhv"):
+                    assert np.array_equal(one[k], singles[l][1][k]), (lanes, l, k)
+
+
 def test_tangent_lanes_zonal_gradient(gpu):
     """The forward-scaling use (solver-2d/examples/m1_forward_scaling.rs):
     P zonal Manning parameters in vertical stripes, all P derivatives in one
