@@ -72,8 +72,9 @@ struct Guard {
   }
 };
 
+// Device buffer of n elements (at least one), not initialised.
 template <class T>
-int calloc_dev(T** p, size_t n) {
+int alloc_dev(T** p, size_t n) {
   if (n == 0) n = 1;
   C_CUDA(cudaMalloc((void**)p, n * sizeof(T)));
   return HF_OK;
@@ -360,23 +361,23 @@ int misfit(hf_calib* c, int64_t run, bool with_tangent_, double* J, double* dJ,
 int alloc_adjoint(hf_calib* c) {
   if (c->seg) return HF_OK;
   const int64_t n_ckpt = (c->K + c->C - 1) / c->C;
-  C_TRY(calloc_dev(&c->ckpt, (size_t)(n_ckpt * 3 * c->ncell)));
-  C_TRY(calloc_dev(&c->seg, (size_t)((2 * c->C + 1) * 3 * c->ncell)));
-  C_TRY(calloc_dev(&c->seg2, (size_t)((2 * c->C + 1) * 3 * c->ncell)));
-  C_TRY(calloc_dev(&c->ctrl_rec, 1));
-  C_TRY(calloc_dev(&c->ctrl_rev, 1));
-  C_TRY(calloc_dev(&c->dh_rev, (size_t)std::max(c->forcing.n_src, 1)));
+  C_TRY(alloc_dev(&c->ckpt, (size_t)(n_ckpt * 3 * c->ncell)));
+  C_TRY(alloc_dev(&c->seg, (size_t)((2 * c->C + 1) * 3 * c->ncell)));
+  C_TRY(alloc_dev(&c->seg2, (size_t)((2 * c->C + 1) * 3 * c->ncell)));
+  C_TRY(alloc_dev(&c->ctrl_rec, 1));
+  C_TRY(alloc_dev(&c->ctrl_rev, 1));
+  C_TRY(alloc_dev(&c->dh_rev, (size_t)std::max(c->forcing.n_src, 1)));
   C_CUDA(cudaStreamCreateWithFlags(&c->s_rec, cudaStreamNonBlocking));
   C_CUDA(cudaStreamCreateWithFlags(&c->s_rev, cudaStreamNonBlocking));
   for (cudaEvent_t* e : {&c->ev_primal, &c->ev_rec[0], &c->ev_rec[1], &c->ev_rev[0], &c->ev_rev[1]})
     C_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
   for (int f = 0; f < 3; ++f) {
-    C_TRY(calloc_dev(&c->lam[f], (size_t)c->ncell));
-    C_TRY(calloc_dev(&c->lam1[f], (size_t)c->ncell));
-    C_TRY(calloc_dev(&c->lamun[f], (size_t)c->ncell));
+    C_TRY(alloc_dev(&c->lam[f], (size_t)c->ncell));
+    C_TRY(alloc_dev(&c->lam1[f], (size_t)c->ncell));
+    C_TRY(alloc_dev(&c->lamun[f], (size_t)c->ncell));
   }
-  C_TRY(calloc_dev(&c->grad, (size_t)c->ncell));
-  C_TRY(calloc_dev(&c->halo, (size_t)c->ntiles * adj_halo_doubles_per_tile()));
+  C_TRY(alloc_dev(&c->grad, (size_t)c->ncell));
+  C_TRY(alloc_dev(&c->halo, (size_t)c->ntiles * adj_halo_doubles_per_tile()));
   return HF_OK;
 }
 
@@ -577,12 +578,12 @@ int alloc_lanes(hf_calib* c, int lanes) {
   free_lanes(c);
   const size_t n = (size_t)lanes * (size_t)c->ncell;
   for (int f = 0; f < 3; ++f) {
-    C_TRY(calloc_dev(&c->dUL[f], n));
-    C_TRY(calloc_dev(&c->dU1L[f], n));
-    if (!c->Ualt[f]) C_TRY(calloc_dev(&c->Ualt[f], (size_t)c->ncell));
+    C_TRY(alloc_dev(&c->dUL[f], n));
+    C_TRY(alloc_dev(&c->dU1L[f], n));
+    if (!c->Ualt[f]) C_TRY(alloc_dev(&c->Ualt[f], (size_t)c->ncell));
   }
-  C_TRY(calloc_dev(&c->dnL, n));
-  C_TRY(calloc_dev(&c->gdhL, (size_t)lanes * (size_t)std::max<int64_t>(c->K * c->G, 1)));
+  C_TRY(alloc_dev(&c->dnL, n));
+  C_TRY(alloc_dev(&c->gdhL, (size_t)lanes * (size_t)std::max<int64_t>(c->K * c->G, 1)));
   c->lanes_cap = lanes;
   return HF_OK;
 }
@@ -735,15 +736,15 @@ int hf_calib_create(const hf_scenario_desc* d, int64_t n_steps, int64_t n_gauges
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
     return bail(ccuda(cudaErrorUnknown, "cudaStreamCreate"));
   for (double** p : {&c->z, &c->n, &c->dn, &c->h0, &c->hu0, &c->hv0})
-    if ((rc = calloc_dev(p, (size_t)ncell))) return bail(rc);
+    if ((rc = alloc_dev(p, (size_t)ncell))) return bail(rc);
   for (int f = 0; f < 3; ++f)
     for (double** p : {&c->U[f], &c->U1[f], &c->dU[f], &c->dU1[f]})
-      if ((rc = calloc_dev(p, (size_t)ncell))) return bail(rc);
+      if ((rc = alloc_dev(p, (size_t)ncell))) return bail(rc);
   const size_t kg = (size_t)(n_steps * n_gauges);
-  if ((rc = calloc_dev(&c->cells, (size_t)n_gauges)) || (rc = calloc_dev(&c->gh, kg)) ||
-      (rc = calloc_dev(&c->gdh, kg)) || (rc = calloc_dev(&c->obs, kg)) ||
-      (rc = calloc_dev(&c->dts, (size_t)n_steps)) || (rc = calloc_dev(&c->ts, (size_t)n_steps)) ||
-      (rc = calloc_dev(&c->ctrl, 1)))
+  if ((rc = alloc_dev(&c->cells, (size_t)n_gauges)) || (rc = alloc_dev(&c->gh, kg)) ||
+      (rc = alloc_dev(&c->gdh, kg)) || (rc = alloc_dev(&c->obs, kg)) ||
+      (rc = alloc_dev(&c->dts, (size_t)n_steps)) || (rc = alloc_dev(&c->ts, (size_t)n_steps)) ||
+      (rc = alloc_dev(&c->ctrl, 1)))
     return bail(rc);
   if (cudaMallocHost((void**)&c->h_ctrl, sizeof(Ctrl)) != cudaSuccess)
     return bail(ccuda(cudaErrorMemoryAllocation, "cudaMallocHost"));
