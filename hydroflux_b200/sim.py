@@ -11,6 +11,8 @@ from __future__ import annotations
 
 import ctypes as C
 import enum
+import os
+import threading
 from dataclasses import dataclass, field
 from typing import Optional, Sequence, Tuple
 
@@ -152,6 +154,31 @@ class SimulationConfig:
                              float(self.friction_dry_tol))
 
 
+_CHECK_POOL = None
+_CHECK_LOCK = threading.Lock()
+_CHECK_WORKERS = max(1, min(8, os.cpu_count() or 1))
+
+
+def _all_nonnegative(a: np.ndarray) -> bool:
+    """a.min() >= 0.0 over the whole field (a NaN fails). Large fields are
+    reduced in contiguous chunks on a few threads (numpy releases the GIL in
+    reductions); each chunk's minimum is tested on its own, so a NaN chunk
+    fails whatever the order."""
+    flat = a.reshape(-1)
+    n = flat.size
+    if n < (1 << 22) or _CHECK_WORKERS == 1:
+        return bool(flat.min() >= 0.0)
+    global _CHECK_POOL
+    with _CHECK_LOCK:
+        if _CHECK_POOL is None:
+            from concurrent.futures import ThreadPoolExecutor
+            _CHECK_POOL = ThreadPoolExecutor(max_workers=_CHECK_WORKERS)
+    k = _CHECK_WORKERS
+    cuts = [n * i // k for i in range(k + 1)]
+    mins = list(_CHECK_POOL.map(lambda i: flat[cuts[i]:cuts[i + 1]].min(), range(k)))
+    return all(bool(m >= 0.0) for m in mins)
+
+
 class Mesh2D:
     """Mesh2D (geometry.rs:31-147). `manning` is a scalar (Mesh2D::new) or a
     field of the bed's shape (Mesh2D::with_manning_field)."""
@@ -173,7 +200,7 @@ class Mesh2D:
             if manning.shape != bed.shape:
                 raise ValueError(f"manning field shape {manning.shape} must match bed shape "
                                  f"{bed.shape}")
-            if not manning.min() >= 0.0:  # a NaN minimum fails too
+            if not _all_nonnegative(manning):  # a NaN fails too
                 raise ValueError("Manning n must be non-negative at every cell")
         self.bed, self.dx, self.dy, self.manning = bed, float(dx), float(dy), manning
 

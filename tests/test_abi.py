@@ -94,6 +94,26 @@ def test_host_validation_without_gpu(libpath):
         assert rc == abi.HF_ERR_INVALID_ARG and b"dx and dy" in lib.hf_last_error()
 
 
+def test_manning_field_check_large(libpath):
+    """Mesh2D::with_manning_field asserts n >= 0 at every cell
+    (geometry.rs:103-106): the mirror's chunked check of a large field
+    rejects a negative or NaN cell wherever it sits, and accepts -0.0."""
+    import numpy as np
+    from hydroflux_b200 import sim
+    n = np.full((2048, 2560), 0.03)  # 5.2 M cells: the threaded path
+    bed = np.zeros_like(n)
+    sim.Mesh2D(bed, 1.0, 1.0, n)
+    flat = n.reshape(-1)
+    for pos in (0, 1, flat.size // 3, flat.size // 2 + 7, flat.size - 1):
+        for bad in (-1e-300, float("nan"), -float("inf")):
+            flat[pos] = bad
+            with pytest.raises(ValueError):
+                sim.Mesh2D(bed, 1.0, 1.0, n)
+        flat[pos] = -0.0
+        sim.Mesh2D(bed, 1.0, 1.0, n)
+        flat[pos] = 0.03
+
+
 def test_python_mirror_errors_without_gpu(libpath):
     import numpy as np
     from hydroflux_b200 import sim
