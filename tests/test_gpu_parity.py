@@ -58,9 +58,10 @@ def random_case(nr, nc, seed, wet=0.7, film=0.05, slope=0.02):
 
 # 20x68 has exactly one tile whose 4-cell halo just fits inside the grid (the
 # interior-tile instantiation at its threshold on all four sides); 20x67 has
-# none; 40x70 and 64x96 mix both kinds.
+# none; 40x70 and 64x96 mix both kinds. 3x40000 and 40000x3 are thin grids of
+# 1,250 and 5,000 tiles, every one of them on two sides.
 SHAPES = [(1, 1), (1, 9), (9, 1), (2, 2), (3, 3), (5, 7), (16, 32), (17, 33), (33, 17),
-          (20, 67), (20, 68), (40, 70), (64, 96)]
+          (20, 67), (20, 68), (40, 70), (64, 96), (3, 40000), (40000, 3)]
 BC_SETS = {
     "walls": ((1, 0),) * 4,
     "trans": ((0, 0),) * 4,
