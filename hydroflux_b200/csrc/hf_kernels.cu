@@ -147,21 +147,49 @@ __global__ void __launch_bounds__(NTHREADS, HF_MIN_BLOCKS)
                   const int* __restrict__ tile_local, const int* __restrict__ n_tiles,
                   int* counter) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  StageSmem& S = *reinterpret_cast<StageSmem*>(smem_raw);
+  StagePfSmem& P = *reinterpret_cast<StagePfSmem*>(smem_raw);
   const int total_tiles = *n_tiles;  // device-resident: a graph serves any set of scenarios
   if (counter == nullptr) {
     for (int t = blockIdx.x; t < total_tiles; t += gridDim.x)
-      batch_tile(args, tile_scn, tile_local, t, S);
+      batch_tile(args, tile_scn, tile_local, t, P.s);
     return;
   }
-  __shared__ int next_tile;
-  while (true) {
-    if (threadIdx.x == 0) next_tile = atomicAdd(counter, 1);
-    __syncthreads();
-    const int t = next_tile;
-    __syncthreads();  // every thread has read next_tile before thread 0 takes another
-    if (t >= total_tiles) break;
-    batch_tile(args, tile_scn, tile_local, t, S);
+  // Dynamic schedule, software-pipelined like k_stage_pf: a CTA claims its
+  // next tile from the counter before it computes the current one, and the
+  // next tile's inputs (of whichever scenario it belongs to) are copied into
+  // shared memory while the current tile's alpha and update phases run.
+  __shared__ int claimed;
+  if (threadIdx.x == 0) claimed = atomicAdd(counter, 1);
+  __syncthreads();
+  int t = claimed;
+  if (t < total_tiles) {
+    const StageArgs& A0 = args[tile_scn[t]];
+    if (A0.ctrl->active) stage_prefetch(A0, P.s, P.hst, tile_local ? tile_local[t] : t - A0.tile_base);
+  }
+  __syncthreads();  // every thread has read `claimed`
+  while (t < total_tiles) {
+    if (threadIdx.x == 0) claimed = atomicAdd(counter, 1);
+    cp_async_wait_all();
+    __syncthreads();  // this tile's inputs are in shared memory; the claim is visible
+    const int tn = claimed;
+    const StageArgs& A = args[tile_scn[t]];
+    const StageArgs* An = tn < total_tiles ? &args[tile_scn[tn]] : nullptr;
+    if (An && !An->ctrl->active) An = nullptr;  // finished scenario: nothing to fetch
+    const int ln = An ? (tile_local ? tile_local[tn] : tn - An->tile_base) : -1;
+    if (A.ctrl->active) {  // uniform over the CTA
+      const int tile = tile_local ? tile_local[t] : t - A.tile_base;
+      double sxm = 0.0, sym = 0.0;
+      unsigned long long nonfin = 0;
+      if (interior_tile(A, tile))
+        stage_tile<double, true, true>(A, P.s, tile, sxm, sym, nonfin, P.hst, ln, An);
+      else
+        stage_tile<double, true>(A, P.s, tile, sxm, sym, nonfin, P.hst, ln, An);
+      if (A.finalize) block_reduce_speeds(sxm, sym, nonfin, A.ctrl);
+    } else if (An) {
+      stage_prefetch(*An, P.s, P.hst, ln);
+    }
+    __syncthreads();  // every thread has read `claimed` before thread 0 takes another
+    t = tn;
   }
 }
 
@@ -535,7 +563,7 @@ int stage_grid_size(int tiles, int device) {
     cudaFuncSetAttribute(k_stage_pf, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)sizeof(StagePfSmem));
     cudaFuncSetAttribute(k_stage_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)sizeof(StageSmem));
+                         (int)sizeof(StagePfSmem));
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stage_pf, NTHREADS,
                                                   sizeof(StagePfSmem));
     if (per_sm < 1) per_sm = 1;
@@ -596,7 +624,7 @@ int launch_finalize_dual(const StageArgs& a, int grid, void* stream, int lanes) 
 
 int launch_stage_batch(const StageArgs* args, const int* tile_scn, const int* n_tiles, int grid,
                        void* stream, const int* tile_local, int* counter) {
-  k_stage_batch<<<grid, NTHREADS, sizeof(StageSmem), (cudaStream_t)stream>>>(
+  k_stage_batch<<<grid, NTHREADS, sizeof(StagePfSmem), (cudaStream_t)stream>>>(
       args, tile_scn, tile_local, n_tiles, counter);
   return cuda_rc(cudaGetLastError());
 }

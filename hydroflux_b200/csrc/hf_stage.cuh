@@ -212,11 +212,14 @@ __device__ __forceinline__ void stage_prefetch(const StageArgs& A, StageSmem& S,
 // With PF (f64 only) the tile's raw inputs are already in shared memory
 // (stage_prefetch into hst, S.eta, S.u, S.v, completed by the caller), and
 // once the faces are done the copies of tile `next` (if >= 0) are started,
-// overlapping the alpha and update phases of this tile.
+// overlapping the alpha and update phases of this tile. `next` is a tile of
+// the grid described by *next_args (another scenario's, in an ensemble), or
+// of A when next_args is null.
 template <class T, bool PF = false, bool IN = false>
 __device__ __forceinline__ void stage_tile_faces(const StageArgs& A, StageSmemT<T>& S, int gi0,
                                                  int gj0, double dt, double* hst = nullptr,
-                                                 int next = -1) {
+                                                 int next = -1,
+                                                 const StageArgs* next_args = nullptr) {
   const int nr = A.nr, nc = A.nc;
   const double dx = A.dx, dy = A.dy;
   const double dt_dx = dt / dx;  // update.rs:930-931
@@ -438,7 +441,8 @@ __device__ __forceinline__ void stage_tile_faces(const StageArgs& A, StageSmemT<
       __syncthreads();
     }
     if constexpr (PF) {
-      if (next >= 0) stage_prefetch(A, S, hst, next);  // eta, u, v and hst are dead now
+      if (next >= 0)  // eta, u, v and hst are dead now
+        stage_prefetch(next_args ? *next_args : A, S, hst, next);
     }
 
     // ---- alpha mass rescaling factors: update.rs:953-982 (tile + 1-cell ring)
@@ -495,7 +499,8 @@ __device__ __forceinline__ void cell_face_beds(const StageArgs& A, const double*
 template <class T, bool PF = false, bool IN = false>
 __device__ __forceinline__ void stage_tile(const StageArgs& A, StageSmemT<T>& S, int tile,
                                            double& sxm, double& sym, unsigned long long& nonfin,
-                                           double* hst = nullptr, int next = -1) {
+                                           double* hst = nullptr, int next = -1,
+                                           const StageArgs* next_args = nullptr) {
   Ctrl* ctrl = A.ctrl;
   const double dt = ctrl->dt;
   const int nr = A.nr, nc = A.nc;
@@ -507,7 +512,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, StageSmemT<T>& S,
   {
     const int tyi = tile / A.tiles_x;
     const int gi0 = tyi * TY, gj0 = (tile - tyi * A.tiles_x) * TX;
-    stage_tile_faces<T, PF, IN>(A, S, gi0, gj0, dt, hst, next);
+    stage_tile_faces<T, PF, IN>(A, S, gi0, gj0, dt, hst, next, next_args);
 
     // ---- FV update + bed source + floor: update.rs:1071-1210
     int src_lo = 0, src_hi = 0;
