@@ -39,6 +39,7 @@ PROTOTYPES = {
     "hf_sim_get_state": (C.c_int, [_VP, _VP, _VP, _VP]),
     "hf_sim_set_state": (C.c_int, [_VP, _VP, _VP, _VP]),
     "hf_sim_get_state_aos": (C.c_int, [_VP, _VP]),
+    "hf_sim_max_depth_exceeds_relief": (C.c_int, [_VP, C.c_double, C.POINTER(C.c_int)]),
     "hf_sim_set_state_aos": (C.c_int, [_VP, _VP]),
     "hf_sim_set_boundaries": (C.c_int, [_VP, C.POINTER(abi.hf_boundaries)]),
     "hf_release_cached_memory": (C.c_int, [C.c_int]),
@@ -100,6 +101,8 @@ PROTOTYPES = {
     "hf_apply_point_sources": (C.c_int, [C.POINTER(abi.hf_grid), _VP, _VP, _VP, C.c_int64,
                                          _I64P, _I64P, _D, C.c_double, _VP]),
     "hf_hllc_flux": (C.c_int, [C.c_int, C.c_int64, _VP, _VP, _VP, _VP]),
+    "hf_max_depth_exceeds_relief": (C.c_int, [C.POINTER(abi.hf_grid), _VP, C.c_double, _VP, _VP,
+                                              C.POINTER(C.c_int)]),
     "hf_ssprk2_step_noalloc": (C.c_int, [C.POINTER(abi.hf_grid), _VP, _VP, _VP,
                                          C.POINTER(abi.hf_boundaries), C.c_double, C.c_int,
                                          _VP]),

@@ -152,11 +152,34 @@ void dfree(void* p) {
   if (p) cudaFree(p);
 }
 
+// max_depth_exceeds_relief (sim.rs:248-271): device max/min reductions, then
+// the reference's host expression on the three values.
+int relief_check(int64_t ncell, const double* h, const double* z, double factor, Ctrl* d_ctrl,
+                 Ctrl* h_ctrl, cudaStream_t st, int* exceeds) {
+  unsigned long long* keys = d_ctrl->relief_keys;
+  HF_CUDA(cudaMemsetAsync(keys, 0, 2 * sizeof(unsigned long long), st));
+  HF_CUDA(cudaMemsetAsync(keys + 2, 0xff, sizeof(unsigned long long), st));
+  if (launch_relief(ncell, h, z, d_ctrl, st)) return cuda_fail(failed_call_error(), "relief");
+  HF_CUDA(cudaMemcpyAsync(h_ctrl->relief_keys, keys, 3 * sizeof(unsigned long long),
+                          cudaMemcpyDeviceToHost, st));
+  HF_CUDA(cudaStreamSynchronize(st));
+  const double max_depth = relief_key_value(h_ctrl->relief_keys[0]);
+  const double bed_max = relief_key_value(h_ctrl->relief_keys[1]);
+  const double bed_min = relief_key_value(h_ctrl->relief_keys[2]);
+  const double relief = std::fmax(bed_max - bed_min, 1.0);  // f64::max(NaN, 1) = 1
+  *exceeds = max_depth > factor * relief ? 1 : 0;
+  return HF_OK;
+}
+
 }  // namespace
 
 int hf::record_error(int code, const char* msg) { return fail(code, msg ? msg : ""); }
 
 BcDev hf::boundaries_dev(const hf_boundaries& b) { return to_bcdev(b); }
+
+int hf::check_boundaries(const hf_boundaries& b, int64_t nr, int64_t nc) {
+  return check_bcs(b, nr, nc);
+}
 
 // ---------------------------------------------------------------- forcing
 void ForcingHost::release_rain() {
@@ -517,26 +540,26 @@ int hf_sim_create(const hf_mesh_desc* mesh, const double* h, const double* hu, c
     return code;
   };
   if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess)
-    return done(cuda_fail(cudaGetLastError(), "cudaStreamCreate"));
+    return done(cuda_fail(failed_call_error(), "cudaStreamCreate"));
   double** bufs[8] = {&s->d_z, &s->d_n, &s->d_h, &s->d_hu, &s->d_hv, &s->d_h1, &s->d_hu1, &s->d_hv1};
   for (double** b : bufs)
     if ((rc = palloc(b, (size_t)ncell, device, s->stream)) != HF_OK) return done(rc);
   // Stream-ordered allocations: usable from any stream once this completes.
   if (cudaStreamSynchronize(s->stream) != cudaSuccess)
-    return done(cuda_fail(cudaGetLastError(), "pool allocation"));
+    return done(cuda_fail(failed_call_error(), "pool allocation"));
   if ((rc = dalloc(&s->d_ctrl, 1)) != HF_OK) return done(rc);
   if (cudaMallocHost((void**)&s->h_ctrl, sizeof(Ctrl)) != cudaSuccess)
-    return done(cuda_fail(cudaGetLastError(), "cudaMallocHost"));
+    return done(cuda_fail(failed_call_error(), "cudaMallocHost"));
   const size_t bytes = (size_t)ncell * sizeof(double);
   if (cudaMemcpy(s->d_z, mesh->bed, bytes, cudaMemcpyHostToDevice) != cudaSuccess)
-    return done(cuda_fail(cudaGetLastError(), "copy bed"));
+    return done(cuda_fail(failed_call_error(), "copy bed"));
   if (mesh->manning) {
     if (cudaMemcpy(s->d_n, mesh->manning, bytes, cudaMemcpyHostToDevice) != cudaSuccess)
-      return done(cuda_fail(cudaGetLastError(), "copy manning"));
+      return done(cuda_fail(failed_call_error(), "copy manning"));
   } else {
     std::vector<double> nn((size_t)ncell, mesh->manning_uniform);
     if (cudaMemcpy(s->d_n, nn.data(), bytes, cudaMemcpyHostToDevice) != cudaSuccess)
-      return done(cuda_fail(cudaGetLastError(), "copy manning"));
+      return done(cuda_fail(failed_call_error(), "copy manning"));
   }
   Ctrl c;
   std::memset(&c, 0, sizeof c);
@@ -544,18 +567,18 @@ int hf_sim_create(const hf_mesh_desc* mesh, const double* h, const double* hu, c
   c.max_dt = cfg->max_dt;
   c.check_finite = cfg->check_finite;
   if (cudaMemcpy(s->d_ctrl, &c, sizeof c, cudaMemcpyHostToDevice) != cudaSuccess)
-    return done(cuda_fail(cudaGetLastError(), "init ctrl"));
+    return done(cuda_fail(failed_call_error(), "init ctrl"));
   if (mesh->manning) {  // n >= 0 at every cell, counted on the device into ctrl.nonfinite
     unsigned long long bad = 0;
     if ((rc = launch_count_bad_manning(ncell, s->d_n, &s->d_ctrl->nonfinite, s->stream)) ||
         cudaMemcpyAsync(&bad, &s->d_ctrl->nonfinite, sizeof bad, cudaMemcpyDeviceToHost,
                         s->stream) != cudaSuccess ||
         cudaStreamSynchronize(s->stream) != cudaSuccess)
-      return done(rc ? fail(rc, "Manning check") : cuda_fail(cudaGetLastError(), "Manning check"));
+      return done(rc ? fail(rc, "Manning check") : cuda_fail(failed_call_error(), "Manning check"));
     if (bad)
       return done(fail(HF_ERR_INVALID_ARG, "Manning n must be non-negative at every cell"));
     if (cudaMemcpy(s->d_ctrl, &c, sizeof c, cudaMemcpyHostToDevice) != cudaSuccess)
-      return done(cuda_fail(cudaGetLastError(), "init ctrl"));
+      return done(cuda_fail(failed_call_error(), "init ctrl"));
   }
   if ((rc = upload3(s, h, hu, hv)) != HF_OK) return done(rc);
   *out = s;
@@ -730,6 +753,14 @@ int hf_sim_set_state(hf_sim* s, const double* h, const double* hu, const double*
   if (!s || !h || !hu || !hv) return fail(HF_ERR_INVALID_ARG, "null argument");
   DeviceGuard guard(s->device);
   return upload3(s, h, hu, hv);
+}
+
+int hf_sim_max_depth_exceeds_relief(hf_sim* s, double factor, int* exceeds) {
+  if (!s || !exceeds) return fail(HF_ERR_INVALID_ARG, "null argument");
+  DeviceGuard guard(s->device);
+  *exceeds = 0;
+  return relief_check(s->nr * s->nc, s->d_h, s->d_z, factor, s->d_ctrl, s->h_ctrl, s->stream,
+                      exceeds);
 }
 
 int hf_sim_get_state_aos(hf_sim* s, double* hhuhv) {
@@ -941,7 +972,7 @@ int hf_workspace_create(int64_t n_rows, int64_t n_cols, int device, hf_workspace
   }
   if (cudaMallocHost((void**)&w->h_ctrl, sizeof(Ctrl)) != cudaSuccess) {
     hf_workspace_destroy(w);
-    return cuda_fail(cudaGetLastError(), "cudaMallocHost");
+    return cuda_fail(failed_call_error(), "cudaMallocHost");
   }
   Ctrl c;
   std::memset(&c, 0, sizeof c);
@@ -1056,6 +1087,17 @@ int hf_cfl_time_step(const hf_grid* grid, const double* h, const double* hu, con
   return HF_OK;
 }
 
+int hf_max_depth_exceeds_relief(const hf_grid* grid, const double* h, double factor,
+                                hf_workspace* w, void* stream, int* exceeds) {
+  HF_TRY(check_grid(grid, w));
+  if (!w || !h || !grid->bed || !exceeds) return fail(HF_ERR_INVALID_ARG, "null argument");
+  DeviceGuard guard(w->device);
+  *exceeds = 0;
+  HF_TRY(relief_check(grid->n_rows * grid->n_cols, h, grid->bed, factor, w->d_ctrl, w->h_ctrl,
+                      (cudaStream_t)stream, exceeds));
+  return HF_OK;
+}
+
 int hf_forward_euler_step(const hf_grid* grid, double* h, double* hu, double* hv,
                           const hf_boundaries* bcs, double dt, hf_workspace* ws, void* stream) {
   return euler_like(grid, h, hu, hv, bcs, dt, ws, stream, false);
@@ -1071,14 +1113,14 @@ int hf_manning_friction_step(const hf_grid* grid, double* h, double* hu, double*
   HF_TRY(check_grid(grid, nullptr));
   if (!grid->manning || !h || !hu || !hv) return fail(HF_ERR_INVALID_ARG, "null buffer");
   return launch_friction(grid->n_rows * grid->n_cols, grid->manning, h, hu, hv, dt, dry_tol,
-                         stream) ? cuda_fail(cudaGetLastError(), "friction") : HF_OK;
+                         stream) ? cuda_fail(failed_call_error(), "friction") : HF_OK;
 }
 
 int hf_apply_rain(int64_t n_cells, double* h, double* hu, double* hv, double rate, double dt,
                   void* stream) {
   if (n_cells < 0 || (n_cells > 0 && (!h || !hu || !hv)))
     return fail(HF_ERR_INVALID_ARG, "bad arguments");
-  return launch_rain(n_cells, h, hu, hv, rate, dt, stream) ? cuda_fail(cudaGetLastError(), "rain")
+  return launch_rain(n_cells, h, hu, hv, rate, dt, stream) ? cuda_fail(failed_call_error(), "rain")
                                                            : HF_OK;
 }
 
@@ -1094,15 +1136,17 @@ int hf_apply_point_sources(const hf_grid* grid, double* h, double* hu, double* h
   if (n_sources > INT_MAX) return fail(HF_ERR_INVALID_ARG, "too many sources");
   return launch_point_sources(grid->n_cols, h, hu, hv, (int)n_sources, rows, cols, q_mass, dt,
                               grid->dx, grid->dy, stream)
-             ? cuda_fail(cudaGetLastError(), "point sources")
+             ? cuda_fail(failed_call_error(), "point sources")
              : HF_OK;
 }
 
 int hf_hllc_flux(int x_dir, int64_t n, const double* ul, const double* ur, double* flux,
                  void* stream) {
   if (n < 0 || (n > 0 && (!ul || !ur || !flux))) return fail(HF_ERR_INVALID_ARG, "bad arguments");
-  return launch_hllc(x_dir, n, ul, ur, flux, stream) ? cuda_fail(cudaGetLastError(), "hllc")
+  return launch_hllc(x_dir, n, ul, ur, flux, stream) ? cuda_fail(failed_call_error(), "hllc")
                                                      : HF_OK;
 }
 
 }  // extern "C"
+
+int hf::check_grid_desc(const hf_grid* g) { return check_grid(g, nullptr); }

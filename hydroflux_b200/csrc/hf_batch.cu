@@ -128,12 +128,12 @@ int enqueue_batch_step(hf_batch* b, int sched) {
   int* c1 = dynamic ? b->d_counters : nullptr;
   int* c2 = dynamic ? b->d_counters + 1 : nullptr;
   if (launch_batch_control(b->d_ctrl, b->d_args1, b->n, b->stream, dynamic ? b->d_counters : nullptr))
-    return bcuda(cudaGetLastError(), "control");
+    return bcuda(failed_call_error(), "control");
   if (launch_stage_batch(b->d_args1, scn, b->d_n_tiles, b->grid, b->stream, local, c1))
-    return bcuda(cudaGetLastError(), "stage 1");
+    return bcuda(failed_call_error(), "stage 1");
   if (launch_stage_batch(b->d_args2, scn, b->d_n_tiles, b->grid, b->stream, local, c2))
-    return bcuda(cudaGetLastError(), "stage 2");
-  if (launch_batch_commit(b->d_ctrl, b->n, b->stream)) return bcuda(cudaGetLastError(), "commit");
+    return bcuda(failed_call_error(), "stage 2");
+  if (launch_batch_commit(b->d_ctrl, b->n, b->stream)) return bcuda(failed_call_error(), "commit");
   return HF_OK;
 }
 
@@ -241,9 +241,9 @@ int hf_batch_create(int64_t n_scenarios, const hf_scenario_desc* sc, int device,
   b->grid = stage_grid_size(b->total_tiles, device);
   b->forcing.resize(b->n);
   if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
-    return done(bcuda(cudaGetLastError(), "cudaStreamCreate"));
+    return done(bcuda(failed_call_error(), "cudaStreamCreate"));
   if (cudaMalloc((void**)&b->buf, 8 * (size_t)total * sizeof(double)) != cudaSuccess)
-    return done(bcuda(cudaGetLastError(), "cudaMalloc(ensemble fields)"));
+    return done(bcuda(failed_call_error(), "cudaMalloc(ensemble fields)"));
   double* f = b->buf;
   b->h = f; b->hu = f + total; b->hv = f + 2 * total; b->h1 = f + 3 * total;
   b->hu1 = f + 4 * total; b->hv1 = f + 5 * total; b->z = f + 6 * total; b->nman = f + 7 * total;
@@ -257,7 +257,7 @@ int hf_batch_create(int64_t n_scenarios, const hf_scenario_desc* sc, int device,
       cudaMalloc((void**)&b->d_counters, 2 * sizeof(int)) != cudaSuccess ||
       cudaMalloc((void**)&b->d_n_tiles, sizeof(int)) != cudaSuccess ||
       cudaMallocHost((void**)&b->h_ctrl, b->n * sizeof(Ctrl)) != cudaSuccess)
-    return done(bcuda(cudaGetLastError(), "cudaMalloc(ensemble tables)"));
+    return done(bcuda(failed_call_error(), "cudaMalloc(ensemble tables)"));
   std::vector<StageArgs> a1(b->n), a2(b->n);
   std::vector<int> tile_scn(b->total_tiles), tile_local(b->total_tiles);
   std::memset(b->h_ctrl, 0, b->n * sizeof(Ctrl));
@@ -275,14 +275,14 @@ int hf_batch_create(int64_t n_scenarios, const hf_scenario_desc* sc, int device,
         cudaMemcpy(b->h + o, d.h, bytes, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(b->hu + o, d.hu, bytes, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(b->hv + o, d.hv, bytes, cudaMemcpyHostToDevice) != cudaSuccess)
-      return done(bcuda(cudaGetLastError(), "upload scenario"));
+      return done(bcuda(failed_call_error(), "upload scenario"));
     if (d.mesh.manning) {
       if (cudaMemcpy(b->nman + o, d.mesh.manning, bytes, cudaMemcpyHostToDevice) != cudaSuccess)
-        return done(bcuda(cudaGetLastError(), "upload manning"));
+        return done(bcuda(failed_call_error(), "upload manning"));
     } else {
       std::vector<double> nn((size_t)ncell, d.mesh.manning_uniform);
       if (cudaMemcpy(b->nman + o, nn.data(), bytes, cudaMemcpyHostToDevice) != cudaSuccess)
-        return done(bcuda(cudaGetLastError(), "upload manning"));
+        return done(bcuda(failed_call_error(), "upload manning"));
     }
     const int tx = (int)((nc + TX - 1) / TX), ty = (int)((nr + TY - 1) / TY);
     int rc = forcing_set_rain(b->forcing[s], d.n_rain, d.rain_t, d.rain_rate);
@@ -353,12 +353,12 @@ int hf_batch_create(int64_t n_scenarios, const hf_scenario_desc* sc, int device,
       cudaMemset(b->d_counters, 0, 2 * sizeof(int)) != cudaSuccess ||
       cudaMemcpy(b->d_n_tiles, &b->total_tiles, sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(b->d_ctrl, b->h_ctrl, b->n * sizeof(Ctrl), cudaMemcpyHostToDevice) != cudaSuccess)
-    return done(bcuda(cudaGetLastError(), "upload ensemble tables"));
+    return done(bcuda(failed_call_error(), "upload ensemble tables"));
   // CFL accumulators of every scenario from its initial state (with ghosts).
   if (launch_cfl_batch(b->d_args1, b->d_tile_scn, 0, b->total_tiles, b->grid, b->stream))
-    return done(bcuda(cudaGetLastError(), "initial CFL"));
+    return done(bcuda(failed_call_error(), "initial CFL"));
   if (cudaStreamSynchronize(b->stream) != cudaSuccess)
-    return done(bcuda(cudaGetLastError(), "initial CFL"));
+    return done(bcuda(failed_call_error(), "initial CFL"));
   *out = b;
   return HF_OK;
 }

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cstring>
 
 #include "../../include/hydroflux_gpu.h"
 #include "hf_arith.h"
@@ -72,6 +73,9 @@ struct Ctrl {
   long long err_step;
   const double* replay_dt;  // MODE_REPLAY
   long long replay_n;
+  // max_depth_exceeds_relief accumulators (order-preserving keys of doubles):
+  // max depth (from 0), max bed, min bed.
+  unsigned long long relief_keys[3];
 };
 
 struct SeriesUnits {
@@ -185,6 +189,15 @@ int launch_point_sources(int64_t nc, double* h, double* hu, double* hv, int n,
                          const int64_t* rows, const int64_t* cols, const double* q, double dt,
                          double dx, double dy, void* stream);
 // *count += cells with !(n >= 0) (count is device memory, zeroed by the caller).
+// max_depth_exceeds_relief reduction (sim.rs:248-271) into c->relief_keys,
+// which the caller presets to {0, 0, ~0}. Decode with relief_key_value.
+int launch_relief(int64_t ncell, const double* h, const double* z, Ctrl* c, void* stream);
+inline double relief_key_value(unsigned long long k) {
+  const unsigned long long b = (k >> 63) ? (k ^ 0x8000000000000000ull) : ~k;
+  double d;
+  std::memcpy(&d, &b, sizeof d);
+  return d;
+}
 int launch_count_bad_manning(int64_t ncell, const double* n, unsigned long long* count,
                              void* stream);
 int launch_hllc(int x_dir, int64_t n, const double* ul, const double* ur, double* out,
@@ -232,7 +245,24 @@ int launch_calib_ckpt(const Ctrl* c, const double* h, const double* hu, const do
 int record_error(int code, const char* msg);
 // Shape, SimulationConfig (sim.rs:130-165) and boundary checks of one grid.
 int check_grid_config(const hf_config* cfg, int64_t nr, int64_t nc);
+// The boundary-set check alone (kinds; Discharge/Depth need >= 2 cells
+// normal to their side) and the low-level grid check (shape; dx, dy > 0 as
+// Mesh2D::new asserts, geometry.rs:59, 93), shared by every entry point.
+int check_boundaries(const hf_boundaries& b, int64_t nr, int64_t nc);
+int check_grid_desc(const hf_grid* g);
 BcDev boundaries_dev(const hf_boundaries& b);
+// The error of this thread's last failed kernel launch in hf_kernels.cu's
+// launchers (they return -7 and keep the cudaError_t here).
+cudaError_t last_launch_error();
+// The error to report once a runtime call or a launcher has failed: the
+// runtime's pending error, else the launch error the launcher consumed, else
+// cudaErrorUnknown, so that a failure is never reported as success.
+inline cudaError_t failed_call_error() {
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const cudaError_t l = last_launch_error();
+  return l != cudaSuccess ? l : cudaErrorUnknown;
+}
 
 // Device copies of one grid's forcing tables (host-side owner).
 struct ForcingHost {

@@ -513,6 +513,37 @@ __global__ void k_count_bad_manning(int64_t ncell, const double* __restrict__ n,
   if ((threadIdx.x & 31) == 0 && bad) atomicAdd(count, bad);
 }
 
+// max_depth_exceeds_relief (sim.rs:248-271): the largest depth folded from
+// 0.0 and the bed's max and min, NaN skipped on every side as f64::max/min
+// do (fmax/fmin return the other operand). Max and min are order-independent,
+// so block partials are combined with atomics on order-preserving keys.
+__device__ __forceinline__ unsigned long long order_key(double x) {
+  const unsigned long long b = (unsigned long long)__double_as_longlong(x);
+  return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+
+__global__ void k_relief(int64_t ncell, const double* __restrict__ h,
+                         const double* __restrict__ z, Ctrl* c) {
+  double hm = 0.0, zmax = -INFINITY, zmin = INFINITY;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < ncell;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    hm = fmax(hm, h[k]);
+    const double zk = z[k];
+    zmax = fmax(zmax, zk);
+    zmin = fmin(zmin, zk);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    hm = fmax(hm, __shfl_xor_sync(0xffffffffu, hm, o));
+    zmax = fmax(zmax, __shfl_xor_sync(0xffffffffu, zmax, o));
+    zmin = fmin(zmin, __shfl_xor_sync(0xffffffffu, zmin, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(&c->relief_keys[0], order_key(hm));
+    atomicMax(&c->relief_keys[1], order_key(zmax));
+    atomicMin(&c->relief_keys[2], order_key(zmin));
+  }
+}
+
 __global__ void k_hllc(int x_dir, int64_t n, const double* ul, const double* ur, double* out) {
   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n;
        k += (int64_t)gridDim.x * blockDim.x) {
@@ -531,7 +562,12 @@ __global__ void k_hllc(int x_dir, int64_t n, const double* ul, const double* ur,
 
 // ------------------------------------------------------------- launchers
 namespace {
-int cuda_rc(cudaError_t e) { return e == cudaSuccess ? 0 : -7; }
+thread_local cudaError_t g_launch_error = cudaSuccess;
+int cuda_rc(cudaError_t e) {
+  if (e == cudaSuccess) return 0;
+  g_launch_error = e;
+  return -7;
+}
 struct DevGuard {
   int prev = -1;
   explicit DevGuard(int dev) {
@@ -550,6 +586,8 @@ int elem_grid(int64_t n) {
   return g < 1 ? 1 : (int)g;
 }
 }  // namespace
+
+cudaError_t last_launch_error() { return g_launch_error; }
 
 size_t stage_smem_bytes() { return sizeof(StageSmem); }
 
@@ -717,6 +755,12 @@ int launch_count_bad_manning(int64_t ncell, const double* n, unsigned long long*
                              void* stream) {
   if (ncell <= 0) return 0;
   k_count_bad_manning<<<elem_grid(ncell), 256, 0, (cudaStream_t)stream>>>(ncell, n, count);
+  return cuda_rc(cudaGetLastError());
+}
+
+int launch_relief(int64_t ncell, const double* h, const double* z, Ctrl* c, void* stream) {
+  if (ncell <= 0) return 0;
+  k_relief<<<elem_grid(ncell), 256, 0, (cudaStream_t)stream>>>(ncell, h, z, c);
   return cuda_rc(cudaGetLastError());
 }
 

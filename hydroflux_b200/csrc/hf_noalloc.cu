@@ -16,7 +16,9 @@
 //     i.e. 24 MiB of stage buffer + 512 B of control block per GPU;
 //   * the first call on a device looks up the array's device address with
 //     cudaGetSymbolAddress (once per device, with that device current);
-//     make that first call before any stream capture;
+//     make that first call before any stream capture. The address is kept
+//     for the life of the process: after cudaDeviceReset on that device it
+//     is stale, and the entry point must not be called again;
 //   * all calls on a device share the one array, which keeps the last call's
 //     contents: calls whose work overlaps on the GPU (other streams, other
 //     host threads) race and corrupt each other, so serialize them;
@@ -51,6 +53,12 @@ double* g_scratch_ptr[64] = {nullptr};
 
 // Message goes to hf_last_error(), like every other entry point.
 int noalloc_fail(int code, const std::string& msg) { return record_error(code, msg.c_str()); }
+
+// The launchers keep the launch's own error (cudaGetLastError has cleared it).
+int launch_failed() {
+  return noalloc_fail(HF_ERR_CUDA, std::string("kernel launch: ") +
+                                       cudaGetErrorString(last_launch_error()));
+}
 
 struct CurrentDevice {
   int prev = -1;
@@ -89,8 +97,6 @@ extern "C" int hf_ssprk2_step_noalloc(const hf_grid* grid, double* h, double* hu
                                       void* stream) {
   if (!grid || !h || !hu || !hv || !grid->bed)
     return noalloc_fail(HF_ERR_INVALID_ARG, "null argument");
-  if (grid->n_rows <= 0 || grid->n_cols <= 0)
-    return noalloc_fail(HF_ERR_SHAPE_MISMATCH, "mesh must have at least one cell");
   if (grid->n_rows > (int64_t)HF_NOALLOC_MAX_CELLS || grid->n_cols > (int64_t)HF_NOALLOC_MAX_CELLS ||
       grid->n_rows * grid->n_cols > (int64_t)HF_NOALLOC_MAX_CELLS) {
     char buf[200];
@@ -101,25 +107,17 @@ extern "C" int hf_ssprk2_step_noalloc(const hf_grid* grid, double* h, double* hu
     return noalloc_fail(HF_ERR_INVALID_ARG, buf);
   }
   if (device < 0 || device >= 64) return noalloc_fail(HF_ERR_INVALID_ARG, "bad device index");
-  // Mesh2D's own checks (geometry.rs:59, 93: dx, dy strictly positive).
-  if (!(grid->dx > 0.0) || !(grid->dy > 0.0))
-    return noalloc_fail(HF_ERR_INVALID_ARG, "dx and dy must be strictly positive");
+  // The same shape, spacing and boundary checks as hf_ssprk2_step.
+  int rc = check_grid_desc(grid);
+  if (rc != HF_OK) return rc;
   hf_boundary t{HF_BC_TRANSMISSIVE, 0, 0.0};
   const hf_boundaries b = bcs ? *bcs : hf_boundaries{t, t, t, t};
-  const hf_boundary* sides[4] = {&b.north, &b.south, &b.west, &b.east};
-  for (int k = 0; k < 4; ++k) {
-    const int kind = sides[k]->kind;
-    if (kind < HF_BC_TRANSMISSIVE || kind > HF_BC_DEPTH)
-      return noalloc_fail(HF_ERR_INVALID_CONFIG, "unknown boundary kind");
-    if ((kind == HF_BC_DISCHARGE || kind == HF_BC_DEPTH) &&
-        (k < 2 ? grid->n_rows : grid->n_cols) < 2)
-      return noalloc_fail(HF_ERR_INVALID_CONFIG,
-                          "Discharge/Depth boundaries need >= 2 cells normal to the side");
-  }
+  rc = check_boundaries(b, grid->n_rows, grid->n_cols);
+  if (rc != HF_OK) return rc;
   CurrentDevice cur(device);
   if (!cur.ok) return noalloc_fail(HF_ERR_CUDA, "cannot make the device current");
   double* base = nullptr;
-  int rc = scratch_on(device, &base);
+  rc = scratch_on(device, &base);
   if (rc != HF_OK) return rc;
   Ctrl* ctrl = reinterpret_cast<Ctrl*>(base);
   double* h1 = base + kCtrlDoubles;
@@ -144,26 +142,20 @@ extern "C" int hf_ssprk2_step_noalloc(const hf_grid* grid, double* h, double* hu
   a.ry = hfa::make_recip(a.dy);
   a.z = grid->bed;
   a.n = grid->manning;
-  for (int k = 0; k < 4; ++k) {
-    a.bc.kind[k] = sides[k]->kind;
-    a.bc.val[k] = sides[k]->value;
-  }
+  a.bc = boundaries_dev(b);
   a.ctrl = ctrl;
   const int gsz = stage_grid_size(a.tiles_x * a.tiles_y, device);
-  if (launch_set_fixed(ctrl, dt, stream))
-    return noalloc_fail(HF_ERR_CUDA, cudaGetErrorString(cudaGetLastError()));
+  if (launch_set_fixed(ctrl, dt, stream)) return launch_failed();
   // Stage 1: U -> scratch (every real cell of h1/hu1/hv1 is written before
   // stage 2 reads it, so the stale stage buffer needs no clearing).
   a.in_h = h; a.in_hu = hu; a.in_hv = hv;
   a.out_h = h1; a.out_hu = hu1; a.out_hv = hv1;
   a.un_h = h; a.un_hu = hu; a.un_hv = hv;
-  if (launch_stage(a, gsz, stream))
-    return noalloc_fail(HF_ERR_CUDA, cudaGetErrorString(cudaGetLastError()));
+  if (launch_stage(a, gsz, stream)) return launch_failed();
   // Stage 2 + convex combination, in place on the caller's state.
   a.in_h = h1; a.in_hu = hu1; a.in_hv = hv1;
   a.out_h = h; a.out_hu = hu; a.out_hv = hv;
   a.combine = 1;
-  if (launch_stage(a, gsz, stream))
-    return noalloc_fail(HF_ERR_CUDA, cudaGetErrorString(cudaGetLastError()));
+  if (launch_stage(a, gsz, stream)) return launch_failed();
   return HF_OK;
 }

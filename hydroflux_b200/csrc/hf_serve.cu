@@ -155,7 +155,7 @@ int enqueue_serve_step(hf_server* v) {
       launch_stage_batch(v->d_args2, v->d_tile_scn, v->d_n_tiles, v->grid, v->stream, nullptr,
                          v->d_counters + 1) ||
       launch_batch_commit(v->d_ctrl, v->max_slots, v->stream))
-    return scuda(cudaGetLastError(), "enqueue serve step");
+    return scuda(failed_call_error(), "enqueue serve step");
   return HF_OK;
 }
 
@@ -219,7 +219,7 @@ int hf_server_create(int device, uint64_t hbm_budget_bytes, int max_slots, hf_se
   v->tile_cap = (int)std::min<uint64_t>(cap, (uint64_t)INT_MAX / 2);
   v->grid = stage_grid_size(std::max(v->tile_cap, 1), device);
   if (cudaStreamCreateWithFlags(&v->stream, cudaStreamNonBlocking) != cudaSuccess)
-    return done(scuda(cudaGetLastError(), "cudaStreamCreate"));
+    return done(scuda(failed_call_error(), "cudaStreamCreate"));
   if (cudaMalloc((void**)&v->d_ctrl, max_slots * sizeof(Ctrl)) != cudaSuccess ||
       cudaMalloc((void**)&v->d_args1, max_slots * sizeof(StageArgs)) != cudaSuccess ||
       cudaMalloc((void**)&v->d_args2, max_slots * sizeof(StageArgs)) != cudaSuccess ||
@@ -227,10 +227,10 @@ int hf_server_create(int device, uint64_t hbm_budget_bytes, int max_slots, hf_se
       cudaMalloc((void**)&v->d_n_tiles, sizeof(int)) != cudaSuccess ||
       cudaMalloc((void**)&v->d_counters, 2 * sizeof(int)) != cudaSuccess ||
       cudaMallocHost((void**)&v->h_ctrl, max_slots * sizeof(Ctrl)) != cudaSuccess)
-    return done(scuda(cudaGetLastError(), "cudaMalloc(server tables)"));
+    return done(scuda(failed_call_error(), "cudaMalloc(server tables)"));
   std::memset(v->h_ctrl, 0, max_slots * sizeof(Ctrl));  // MODE_FIXED: empty
   if (cudaMemcpy(v->d_ctrl, v->h_ctrl, max_slots * sizeof(Ctrl), cudaMemcpyHostToDevice) != cudaSuccess)
-    return done(scuda(cudaGetLastError(), "init slots"));
+    return done(scuda(failed_call_error(), "init slots"));
   int rc = rebuild_tiles(v);
   if (rc != HF_OK) return done(rc);
   *out = v;
@@ -293,14 +293,14 @@ int hf_server_admit(hf_server* v, const hf_scenario_desc* d, int* slot_out) {
       cudaMemcpy(h, d->h, fb, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(hu, d->hu, fb, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(hv, d->hv, fb, cudaMemcpyHostToDevice) != cudaSuccess)
-    return undo(scuda(cudaGetLastError(), "upload scenario"));
+    return undo(scuda(failed_call_error(), "upload scenario"));
   if (d->mesh.manning) {
     if (cudaMemcpy(nm, d->mesh.manning, fb, cudaMemcpyHostToDevice) != cudaSuccess)
-      return undo(scuda(cudaGetLastError(), "upload manning"));
+      return undo(scuda(failed_call_error(), "upload manning"));
   } else {
     std::vector<double> nn((size_t)ncell, d->mesh.manning_uniform);
     if (cudaMemcpy(nm, nn.data(), fb, cudaMemcpyHostToDevice) != cudaSuccess)
-      return undo(scuda(cudaGetLastError(), "upload manning"));
+      return undo(scuda(failed_call_error(), "upload manning"));
   }
   int rc = forcing_set_rain(s.forcing, d->n_rain, d->rain_t, d->rain_rate);
   if (rc == HF_OK)
@@ -343,7 +343,7 @@ int hf_server_admit(hf_server* v, const hf_scenario_desc* d, int* slot_out) {
   c.budget = d->cfg.max_steps > (uint64_t)LLONG_MAX ? LLONG_MAX : (long long)d->cfg.max_steps;
   v->h_ctrl[k] = c;
   if (cudaMemcpy(v->d_ctrl + k, &c, sizeof c, cudaMemcpyHostToDevice) != cudaSuccess)
-    return undo(scuda(cudaGetLastError(), "init slot"));
+    return undo(scuda(failed_call_error(), "init slot"));
   rc = rebuild_tiles(v);
   if (rc != HF_OK) {
     undo(rc);
@@ -355,7 +355,7 @@ int hf_server_admit(hf_server* v, const hf_scenario_desc* d, int* slot_out) {
   if (launch_cfl_batch(v->d_args1, v->d_tile_scn, tb, tb + s.tiles_x * s.tiles_y, v->grid,
                        v->stream) ||
       cudaStreamSynchronize(v->stream) != cudaSuccess)
-    return scuda(cudaGetLastError(), "initial CFL");
+    return scuda(failed_call_error(), "initial CFL");
   v->in_use += bytes;
   *slot_out = k;
   return HF_OK;

@@ -345,6 +345,14 @@ class Simulation:
         raise_for(lib().hf_sim_get_state(self._h, h.ctypes.data, hu.ctypes.data, hv.ctypes.data))
         return h, hu, hv
 
+    def max_depth_exceeds_relief(self, factor: float) -> bool:
+        """max_depth_exceeds_relief(sim.states(), sim.mesh(), factor)
+        (sim.rs:248-271): whether the largest depth exceeds `factor` times
+        the bed's relief (floored at 1 m), reduced on the device."""
+        out = C.c_int()
+        raise_for(lib().hf_sim_max_depth_exceeds_relief(self._h, float(factor), C.byref(out)))
+        return bool(out.value)
+
     def set_states(self, states) -> None:
         h, hu, hv = _split_states(states, self._shape)
         raise_for(lib().hf_sim_set_state(self._h, h.ctypes.data, hu.ctypes.data, hv.ctypes.data))

@@ -2,8 +2,9 @@
 
 Mirrors solver-2d's re-exports (lib.rs:74-91): `cfl_time_step`,
 `cfl_time_step_with_bcs`, `forward_euler_step(_with)`, `ssprk2_step(_with)`,
-`manning_friction_step`, `apply_rain`, `apply_point_sources`, and the
-`StepWorkspace2D` scratch object. Arrays are float64 CUDA tensors of shape
+`manning_friction_step`, `apply_rain`, `apply_point_sources`,
+`max_depth_exceeds_relief` (sim.rs:262), and the `StepWorkspace2D` scratch
+object. Arrays are float64 CUDA tensors of shape
 (n_rows, n_cols); steps mutate h/hu/hv in place on torch's current stream.
 Shape mismatches raise ValueError where the reference panics.
 """
@@ -141,6 +142,18 @@ def manning_friction_step(h, hu, hv, mesh: DeviceMesh, dt: float, dry_tol: float
                                              _check(hu, mesh.shape, "hu"),
                                              _check(hv, mesh.shape, "hv"), float(dt),
                                              float(dry_tol), _stream()))
+
+
+def max_depth_exceeds_relief(h, mesh: DeviceMesh, factor: float,
+                             ws: Optional[StepWorkspace2D] = None) -> bool:
+    """max_depth_exceeds_relief (sim.rs:248-271) on a device depth field."""
+    ws = ws or StepWorkspace2D(*mesh.shape)
+    g = mesh.grid()
+    out = C.c_int()
+    raise_for(lib().hf_max_depth_exceeds_relief(C.byref(g), _check(h, mesh.shape, "h"),
+                                                float(factor), ws.handle(), _stream(),
+                                                C.byref(out)))
+    return bool(out.value)
 
 
 def apply_rain(h, hu, hv, rate: float, dt: float):

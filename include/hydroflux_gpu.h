@@ -151,6 +151,9 @@ int hf_sim_time(const hf_sim* sim, double* t);
 int hf_sim_steps(const hf_sim* sim, uint64_t* steps);
 /* Simulation::states / states_mut (sim.rs:177-186): host copies. */
 int hf_sim_get_state(hf_sim* sim, double* h, double* hu, double* hv);
+/* max_depth_exceeds_relief(sim.states(), sim.mesh(), factor) (sim.rs:262):
+ * the same check on the simulation's current state and bed, on its stream. */
+int hf_sim_max_depth_exceeds_relief(hf_sim* sim, double factor, int* exceeds);
 int hf_sim_set_state(hf_sim* sim, const double* h, const double* hu, const double* hv);
 int hf_sim_get_state_aos(hf_sim* sim, double* hhuhv);
 int hf_sim_set_state_aos(hf_sim* sim, const double* hhuhv);
@@ -410,6 +413,14 @@ int hf_apply_rain(int64_t n_cells, double* h, double* hu, double* hv, double rat
 int hf_apply_point_sources(const hf_grid* grid, double* h, double* hu, double* hv,
                            int64_t n_sources, const int64_t* rows, const int64_t* cols,
                            const double* q_mass, double dt, void* stream);
+/* max_depth_exceeds_relief (sim.rs:248-271): the reference's plausibility
+ * check for a finite blow-up. *exceeds = 1 when the largest depth (folded
+ * from 0, NaN skipped) exceeds factor * max(bed.max() - bed.min(), 1 m),
+ * else 0. The max/min reductions run on the device over h and the bed
+ * (device arrays of the grid's shape); the workspace supplies the
+ * accumulators and the pinned readback. Synchronizes `stream`. */
+int hf_max_depth_exceeds_relief(const hf_grid* grid, const double* h, double factor,
+                                hf_workspace* ws, void* stream, int* exceeds);
 /* ssprk2_step without allocating: no counterpart in the reference (whose
  * StepWorkspace2D is always caller-allocated host memory). Same result as
  * hf_ssprk2_step, but the stage buffer and control block live in a fixed
@@ -423,7 +434,9 @@ int hf_apply_point_sources(const hf_grid* grid, double* h, double* hu, double* h
  *   until the process exits.
  * - The first call on a device resolves the array's device address
  *   (cudaGetSymbolAddress, with `device` current); make that first call
- *   before any stream capture.
+ *   before any stream capture. The address is kept for the life of the
+ *   process: after cudaDeviceReset on that device it is stale, so do not
+ *   call this entry point again in that process.
  * - All calls on a device share the array and see the previous call's
  *   leftovers (the control block is cleared each call): calls whose GPU work
  *   overlaps, e.g. on two streams, race. Serialize them. */

@@ -178,6 +178,18 @@ def apply_point_sources(h, hu, hv, sources, dt, dx, dy):
     return h, hu, hv
 
 
+def max_depth_exceeds_relief(h, z, factor):
+    """max_depth_exceeds_relief (solver-2d/src/sim.rs:262-271), restated:
+    the depth max folds from 0.0 and the bed's max/min from -inf/+inf with
+    f64::max/min, which skip NaN (np.fmax/np.fmin do the same); the relief
+    is floored at 1 m with f64::max (NaN gives 1)."""
+    max_depth = float(np.fmax.reduce(np.ravel(h), initial=0.0))
+    bed_max = float(np.fmax.reduce(np.ravel(z), initial=-np.inf))
+    bed_min = float(np.fmin.reduce(np.ravel(z), initial=np.inf))
+    relief = float(np.fmax(bed_max - bed_min, 1.0))
+    return max_depth > factor * relief
+
+
 def series_eval(t, v, x):
     t, v = _f64(t), _f64(v)
     return lib().hfo_series_eval(_p(t), _p(v), C.c_int64(len(t)), C.c_double(x))

@@ -1,7 +1,7 @@
 """Forcing-series units and control-point gauges on the GPU, bitwise against
-the oracle; and the LISFLOOD-FP benchmark decks on real terrain (when a copy
-of the decks is named by HYDROFLUX_UK_EA_DIR), GPU against the oracle over
-the first steps of each event."""
+the oracle; and the LISFLOOD-FP benchmark decks on real terrain (the
+committed tests/golden/uk_ea fixtures), GPU against the oracle over the
+first steps of each event."""
 import os
 
 import numpy as np
@@ -152,7 +152,11 @@ def test_gauge_errors(gpu):
             s.gauge_peaks()
 
 
-UK_EA = os.environ.get("HYDROFLUX_UK_EA_DIR")
+# The decks are committed as fixtures (tests/golden/uk_ea, copied from the
+# reference's benchmarks/data/uk_ea by tests/golden/make_golden.py);
+# HYDROFLUX_UK_EA_DIR may name another copy.
+UK_EA = os.environ.get("HYDROFLUX_UK_EA_DIR") or os.path.join(
+    os.path.dirname(os.path.abspath(__file__)), "golden", "uk_ea")
 DECKS = [("test8a_glasgow/ea8-2m.par", None, 10.0, 1500),
          ("test4/ea4.par", "ea4-5m.dem", 15.0, 1500)]
 
@@ -162,8 +166,7 @@ def test_real_terrain_decks(gpu, oracle, deck, dem, max_dt, n_steps):
     """The UK EA decks (urban rain + point inflow on a 481 x 199 DEM; line
     inflow over a 400 x 200 floodplain), first steps of each event, GPU
     against the oracle bitwise, gauges included."""
-    if not UK_EA or not os.path.exists(os.path.join(UK_EA, deck)):
-        pytest.skip("HYDROFLUX_UK_EA_DIR does not hold the decks")
+    assert os.path.exists(os.path.join(UK_EA, deck)), f"deck fixture missing under {UK_EA}"
     sim, L = gpu
     case = L.load_case(os.path.join(UK_EA, deck), dem=dem, max_dt=max_dt)
     s = L.simulation(case)

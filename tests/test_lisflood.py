@@ -6,8 +6,9 @@ import os
 import numpy as np
 import pytest
 
-REF_DATA = os.environ.get("HYDROFLUX_REFERENCE_DIR", "/root/reference")
-UK_EA = os.path.join(REF_DATA, "benchmarks/data/uk_ea")
+# The two UK EA decks are committed as fixtures (copied from the reference's
+# benchmarks/data/uk_ea by tests/golden/make_golden.py).
+UK_EA = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "uk_ea")
 
 
 @pytest.fixture(scope="module")
@@ -149,8 +150,6 @@ def test_oracle_units_match_example_arithmetic(L, tmp_path, oracle):
 @pytest.mark.parametrize("deck", ["test8a_glasgow/ea8-2m.par", "test4/ea4.par"])
 def test_reference_decks(L, deck):
     path = os.path.join(UK_EA, deck)
-    if not os.path.exists(path):
-        pytest.skip("reference data not present")
     if deck.startswith("test8a"):
         c = L.load_case(path, max_dt=10.0)
         assert c.mesh.bed.shape == (199, 481) and len(c.gauges) == 9 and len(c.sources) == 1

@@ -433,3 +433,33 @@ def test_both_pow_modes_reproduce_reference_profiles(oracle, mode):
     finally:
         oracle.set_pow_mode("libm")
     assert np.array_equal(cases.golden_profile(c, h), golden["macdonald"])
+
+
+def test_max_depth_exceeds_relief_flags_a_finite_blow_up(oracle):  # sim.rs:376-386
+    bed = np.repeat(np.arange(4, dtype=float)[:, None] * 32.0, 4, axis=1)  # 0..96 m
+    assert not oracle.max_depth_exceeds_relief(np.full((4, 4), 5.0), bed, 3.0)
+    assert oracle.max_depth_exceeds_relief(np.full((4, 4), 3000.0), bed, 3.0)
+
+
+def test_max_depth_exceeds_relief_floors_a_near_flat_mesh(oracle):  # sim.rs:388-397
+    bed = np.zeros((3, 3))
+    assert not oracle.max_depth_exceeds_relief(np.full((3, 3), 2.0), bed, 3.0)
+    assert oracle.max_depth_exceeds_relief(np.full((3, 3), 50.0), bed, 3.0)
+
+
+def test_max_depth_exceeds_relief_fold_semantics(oracle):
+    """The folds of sim.rs:263-265: NaN depths and beds are skipped, the
+    depth max starts at 0 (all-negative or all-NaN depths give 0), and a
+    relief below 1 m or NaN takes the 1 m floor (an all-NaN bed gives
+    -inf - inf = -inf, an all-inf bed inf - inf = NaN, and NaN.max(1.0)
+    is 1.0)."""
+    bed = np.array([[0.0, np.nan], [4.0, 1.0]])
+    h = np.array([[np.nan, 11.9], [-3.0, np.nan]])
+    assert not oracle.max_depth_exceeds_relief(h, bed, 3.0)   # 11.9 <= 12
+    h[0, 0] = 12.5
+    assert oracle.max_depth_exceeds_relief(h, bed, 3.0)
+    assert not oracle.max_depth_exceeds_relief(np.full((2, 2), np.nan), bed, 0.0)  # 0 > 0 is false
+    assert oracle.max_depth_exceeds_relief(np.full((2, 2), 1.5), np.full((2, 2), np.nan), 1.0)
+    assert oracle.max_depth_exceeds_relief(np.full((2, 2), 1.5), np.full((2, 2), np.inf), 1.0)
+    inf_bed = np.array([[0.0, np.inf], [1.0, 2.0]])  # infinite relief
+    assert not oracle.max_depth_exceeds_relief(np.full((2, 2), 1e300), inf_bed, 1.0)

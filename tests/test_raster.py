@@ -23,7 +23,10 @@ SAMPLE = ("ncols         4\n"
           "5 6 7 8\n"
           "9 10 11 12\n")
 
-REF_DATA = os.environ.get("HYDROFLUX_REFERENCE_DIR", "/root/reference")
+# A checkout of the reference, when one is named, adds its Huasco result grid;
+# the Test 8A grids are committed fixtures (tests/golden/uk_ea).
+REF_DATA = os.environ.get("HYDROFLUX_REFERENCE_DIR")
+UK_EA = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "uk_ea")
 
 
 @pytest.fixture(scope="module")
@@ -338,17 +341,20 @@ def test_mesh_builders(R, tmp_path):
 # --- the reference's own data files ------------------------------------------
 
 REF_GRIDS = [
-    "examples/huasco_2d_phase2/data/synxflow_noflow_h_86400.asc.gz",
-    "benchmarks/data/uk_ea/test8a_glasgow/ea8-2m.dem.gz",
-    "benchmarks/data/uk_ea/test8a_glasgow/ea8-2m.n.gz",
+    ("reference", "examples/huasco_2d_phase2/data/synxflow_noflow_h_86400.asc.gz"),
+    ("fixture", "test8a_glasgow/ea8-2m.dem.gz"),
+    ("fixture", "test8a_glasgow/ea8-2m.n.gz"),
 ]
 
 
-@pytest.mark.parametrize("rel", REF_GRIDS)
-def test_reference_data_files(R, rel):
-    path = os.path.join(REF_DATA, rel)
-    if not os.path.exists(path):
-        pytest.skip("reference data not present")
+@pytest.mark.parametrize("where,rel", REF_GRIDS)
+def test_reference_data_files(R, where, rel):
+    if where == "reference":
+        if not REF_DATA or not os.path.exists(os.path.join(REF_DATA, rel)):
+            pytest.skip("HYDROFLUX_REFERENCE_DIR does not name a reference checkout")
+        path = os.path.join(REF_DATA, rel)
+    else:
+        path = os.path.join(UK_EA, rel)
     data, h = check_against_oracle(R, path)
     assert data.shape == (h.nrows, h.ncols) and np.all(np.isfinite(data))
 
@@ -358,9 +364,7 @@ def test_reference_urban_grids(R):
     uk_ea_test8a_official.rs): a 481 x 199 DEM at 2 m without NODATA, a
     Manning grid of the same geometry with two values, and every control
     point and the inflow point inside the grid."""
-    d = os.path.join(REF_DATA, "benchmarks/data/uk_ea/test8a_glasgow")
-    if not os.path.exists(os.path.join(d, "ea8-2m.dem.gz")):
-        pytest.skip("reference data not present")
+    d = os.path.join(UK_EA, "test8a_glasgow")
     mesh, h = R.mesh_from_ascii_grid(os.path.join(d, "ea8-2m.dem.gz"),
                                      os.path.join(d, "ea8-2m.n.gz"))
     assert (h.nrows, h.ncols, h.cellsize) == (199, 481, 2.0)

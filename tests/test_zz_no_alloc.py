@@ -34,7 +34,9 @@ def _case(nr, nc, seed):
     return z, h, hu, hv
 
 
-@pytest.mark.parametrize("shape", [(37, 53), (512, 512)])
+# (1024, 1024) is exactly HF_NOALLOC_MAX_CELLS: its stage buffer reaches the
+# last element of the fixed scratch array.
+@pytest.mark.parametrize("shape", [(37, 53), (512, 512), (1024, 1024)])
 def test_noalloc_step_matches_workspace_step(torch_cuda, shape):
     torch = torch_cuda
     from hydroflux_b200 import sim, step
