@@ -238,7 +238,7 @@ HF_ADJ_HD void ghost_rev(int side, const BcDev& bc, double h,
       const double h_n = hfpow::pow_3_5(x);
       const double w = h_n < DRY_INFLOW_H_MAX ? 1.0 : (DRY_INFLOW_H_MAX < h_n ? 0.0 : 0.5);
       const double e = 3.0 / 5.0;
-      Ln += LGh * w * (e * pow(x, e - 1.0)) * qs;
+      Ln += LGh * w * (e * hfpow::pow_libm(x, e - 1.0)) * qs;
     }
   }
   if (h_from_cell) Lh += LGh;

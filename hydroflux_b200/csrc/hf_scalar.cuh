@@ -104,17 +104,17 @@ __device__ __forceinline__ DualD r_min(DualD a, DualD b) {
   return DualD{a.v, 0.5 * (a.d + b.d)};
 }
 
-// x^fl(4/3), x^fl(3/5) (dual.rs:112-117: dval = n * val^(n-1) * dval); the
-// value is the correctly rounded power.
+// x^fl(4/3), x^fl(3/5) (dual.rs:112-117: dval = n * val^(n-1) * dval), every
+// power rounded as the host libm's pow rounds it (hf_pow.h).
 __device__ __forceinline__ double r_pow43(double x) { return hfpow::pow_4_3(x); }
 __device__ __forceinline__ double r_pow35(double x) { return hfpow::pow_3_5(x); }
 __device__ __forceinline__ DualD r_pow43(DualD x) {
   const double n = 4.0 / 3.0;
-  return DualD{hfpow::pow_4_3(x.v), n * pow(x.v, n - 1.0) * x.d};
+  return DualD{hfpow::pow_4_3(x.v), n * hfpow::pow_libm(x.v, n - 1.0) * x.d};
 }
 __device__ __forceinline__ DualD r_pow35(DualD x) {
   const double n = 3.0 / 5.0;
-  return DualD{hfpow::pow_3_5(x.v), n * pow(x.v, n - 1.0) * x.d};
+  return DualD{hfpow::pow_3_5(x.v), n * hfpow::pow_libm(x.v, n - 1.0) * x.d};
 }
 
 // Loads / stores of a field held as value and (optional) tangent arrays.

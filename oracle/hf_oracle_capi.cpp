@@ -178,14 +178,30 @@ int hfo_set_threads(int n) {
 #endif
 }
 
-// 0: libm pow (the reference's platform behaviour); 1: correctly rounded.
+// 0: libm pow (the reference's platform behaviour); 1: its restatement
+// (hf_pow.h, the GPU's pow).
 int hfo_set_pow_mode(int mode) {
   pow_mode() = mode ? 1 : 0;
   return pow_mode();
 }
 
-double hfo_pow_cr(double x, int which) {
-  return which == 0 ? hfpow::pow_4_3(x) : hfpow::pow_3_5(x);
+double hfo_pow_port(double x, double y) { return hfpow::pow_libm(x, y); }
+
+// Counts the x[k] (k < n) whose x^y differs, bit for bit, between the
+// restatement and the host libm; the first few go to first_bad (up to 8).
+int64_t hfo_pow_mismatches(int64_t n, const double* x, double y, double* first_bad) {
+  int64_t bad = 0;
+  for (int64_t k = 0; k < n; ++k) {
+    const double a = hfpow::pow_libm(x[k], y), b = std::pow(x[k], y);
+    uint64_t ba, bb;
+    std::memcpy(&ba, &a, 8);
+    std::memcpy(&bb, &b, 8);
+    if (ba != bb && !(a != a && b != b)) {
+      if (first_bad && bad < 8) first_bad[bad] = x[k];
+      ++bad;
+    }
+  }
+  return bad;
 }
 
 int hfo_get_threads(void) {

@@ -36,8 +36,10 @@ def lib():
         _LIB = C.CDLL(path)
         _LIB.hfo_last_error.restype = C.c_char_p
         _LIB.hfo_series_eval.restype = C.c_double
-        _LIB.hfo_pow_cr.restype = C.c_double
-        _LIB.hfo_pow_cr.argtypes = [C.c_double, C.c_int]
+        _LIB.hfo_pow_port.restype = C.c_double
+        _LIB.hfo_pow_port.argtypes = [C.c_double, C.c_double]
+        _LIB.hfo_pow_mismatches.restype = C.c_int64
+        _LIB.hfo_pow_mismatches.argtypes = [C.c_int64, C.c_void_p, C.c_double, C.c_void_p]
         _LIB.hfo_set_series_units.restype = None
         _LIB.hfo_set_series_units.argtypes = [C.c_double] * 6
         _LIB.hfo_set_gauges.restype = None
@@ -46,14 +48,26 @@ def lib():
 
 
 def set_pow_mode(mode: str) -> None:
-    """'libm' (the reference's platform pow, default) or 'cr' (correctly
-    rounded x^fl(4/3) and x^fl(3/5), as the GPU kernels compute)."""
-    lib().hfo_set_pow_mode(1 if mode == "cr" else 0)
+    """'libm' (the host C library's pow, which the Rust reference's
+    f64::powf calls; default) or 'port' (the restatement of that library's
+    algorithm in hydroflux_b200/csrc/hf_pow.h, which the GPU runs)."""
+    if mode not in ("libm", "port"):
+        raise ValueError(f"unknown pow mode {mode!r}")
+    lib().hfo_set_pow_mode(1 if mode == "port" else 0)
 
 
-def pow_cr(x: float, which: int) -> float:
-    """Correctly rounded x^fl(4/3) (which = 0) or x^fl(3/5) (which = 1)."""
-    return lib().hfo_pow_cr(float(x), int(which))
+def pow_port(x: float, y: float) -> float:
+    """x^y by the restatement in hf_pow.h (host build)."""
+    return lib().hfo_pow_port(float(x), float(y))
+
+
+def pow_mismatches(x, y: float):
+    """(count, first few x) of the x whose x^y differs bit for bit between
+    the restatement and the host libm."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    first = np.full(8, np.nan)
+    n = lib().hfo_pow_mismatches(x.size, x.ctypes.data, float(y), first.ctypes.data)
+    return int(n), first[:min(int(n), 8)]
 
 
 class OracleError(RuntimeError):

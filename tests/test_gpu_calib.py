@@ -3,7 +3,7 @@
 * The DualD tangent reproduces the reference's published forward-mode
   calibration record (m1_inverse_manning_demo.rs; 12 Newton iterations).
 * The tangent equals the oracle's Dual tangent over the same dt sequence:
-  the misfit J bit for bit (cr pow mode), dJ and the final tangent state to
+  the misfit J bit for bit, dJ and the final tangent state to
   1e-10.
 * The adjoint is the transpose of the tangent: for random directions in the
   Manning field and the initial state, dot(gradient, direction) equals the
@@ -37,10 +37,9 @@ def gpu():
 
 
 @pytest.fixture(autouse=True)
-def cr_pow(oracle):
-    oracle.set_pow_mode("cr")
-    yield
+def libm_pow(oracle):
     oracle.set_pow_mode("libm")
+    yield
 
 
 def m1_scenario(workloads, n_value):
@@ -59,7 +58,6 @@ def test_tangent_matches_reference_newton_record(gpu):
             st = cal.final_state()
             return cases.m1_centroid(st["h"][1], st["dh"][1])
         rows, _ = cases.m1_newton(centroid)
-    # The kernels' pow is correctly rounded, the reference's is the platform's.
     cases.assert_matches_m1_record(rows, np.load(GOLDEN)["table"], dc=5e-12)
 
 

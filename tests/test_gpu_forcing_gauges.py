@@ -22,10 +22,9 @@ def gpu():
 
 
 @pytest.fixture(autouse=True)
-def cr_pow(oracle):
-    oracle.set_pow_mode("cr")
-    yield
+def libm_pow(oracle):
     oracle.set_pow_mode("libm")
+    yield
     oracle.Forcing().args()  # default series units
 
 

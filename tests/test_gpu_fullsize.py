@@ -1,8 +1,9 @@
 """The benchmark's 4096 x 4096 valley at full size.
 
-* Two SSP-RK2 steps (rain, point inflow, Manning friction, transmissive
-  sides) from a wet, warmed state: the GPU against the oracle bit for bit,
-  16.8 M cells, the same dt sequence.
+* Twelve SSP-RK2 steps (rain, point inflow, Manning friction, transmissive
+  sides) from the dry start, through the wetting of every cell: the GPU
+  against the oracle (host libm pow) bit for bit, 16.8 M cells, the same dt
+  sequence.
 * The batched stage (an ensemble of this one scenario) against the
   single-grid stage on the same input, bit for bit: two different kernels
   and tile schedules over every interior and edge tile of the grid.
@@ -45,26 +46,35 @@ def warmed(gpu):
     return dataclasses.replace(scn, h=h, hu=hu, hv=hv)
 
 
-def test_two_steps_bitwise_against_oracle(gpu, oracle, warmed):
+def test_dry_start_bitwise_against_oracle(gpu, oracle):
+    """The workload from its dry start at t = 0: rain (50 mm/h) and the
+    inflow hydrograph wet the dry valley, so the first steps cross the dry
+    and velocity thresholds in every cell. After 1, 4 and 12 steps the GPU
+    equals the oracle (the host libm's pow, the reference's arithmetic) bit
+    for bit, with the same clock."""
     _, workloads, ensemble = gpu
-    s = warmed
-    assert float((s.h > 1e-6).mean()) > 0.99  # the wet path runs everywhere
-    with workloads.simulation_for(s) as sm:
-        sm.run_steps(2, s.t_end)
-        got = sm.states()
-        steps, t = sm.steps(), sm.time()
+    scn = workloads.valley(n=N, dx=5.0, seed=0)
+    assert float(np.max(scn.h)) == 0.0  # dry start
+    cfg = ensemble.scenario_config(scn)
+    forcing = workloads.oracle_forcing(scn)
     threads = oracle.get_threads()
-    oracle.set_pow_mode("cr")
+    oracle.set_pow_mode("libm")
     oracle.set_threads(os.cpu_count() or 1)
     try:
-        r = oracle.sim_run(s.bed, s.manning, s.dx, s.dy, s.h, s.hu, s.hv,
-                           ensemble.scenario_config(s), s.t_end,
-                           forcing=workloads.oracle_forcing(s), stop_after=2)
+        state, t0, k0 = (scn.h, scn.hu, scn.hv), 0.0, 0
+        with workloads.simulation_for(scn) as sm:
+            for k in (1, 4, 12):
+                sm.run_steps(k - sm.steps(), scn.t_end)
+                got = sm.states()
+                r = oracle.sim_run(scn.bed, scn.manning, scn.dx, scn.dy, *state, cfg, scn.t_end,
+                                   forcing=forcing, stop_after=k - k0, t0=t0, steps0=k0)
+                assert r["status"] == 0 and r["steps"] == sm.steps() == k
+                assert r["t"] == sm.time()
+                assert exact_fraction(got, (r["h"], r["hu"], r["hv"])) == 1.0, f"after {k} steps"
+                state, t0, k0 = (r["h"], r["hu"], r["hv"]), r["t"], r["steps"]
+        assert float((state[0] > 1e-6).mean()) > 0.99  # every cell wetted
     finally:
         oracle.set_threads(threads)
-        oracle.set_pow_mode("libm")
-    assert r["status"] == 0 and r["steps"] == steps == 2 and r["t"] == t
-    assert exact_fraction(got, (r["h"], r["hu"], r["hv"])) == 1.0
 
 
 def test_batched_stage_matches_single_grid_stage(gpu, warmed):

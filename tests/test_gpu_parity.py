@@ -30,11 +30,11 @@ def gpu():
 
 
 @pytest.fixture(autouse=True)
-def cr_pow(oracle):
-    """The kernels raise to 4/3 and 3/5 with a correctly rounded pow; the
-    oracle does the same here, so every comparison below is bitwise. Tests
-    that check against the platform libm pow switch back explicitly."""
-    oracle.set_pow_mode("cr")
+def libm_pow(oracle):
+    """The kernels raise to 4/3 and 3/5 with a pow that rounds as the host
+    libm does (hf_pow.h); the oracle calls that libm (its default mode), so
+    every comparison below is bitwise against the reference's arithmetic."""
+    oracle.set_pow_mode("libm")
     yield
     oracle.set_pow_mode("libm")
 
@@ -106,8 +106,8 @@ def test_step_parity_random(gpu, oracle, shape, bcname, integrator):
             step.ssprk2_step(dh, dhu, dhv, mesh, bcs_obj(sim, pairs), dt, ws)
         got = to_host(dh, dhu, dhv)
         assert_parity(got, ref, what=f"step {it}: ")
-        # Every operation is IEEE-rounded or (pow) correctly rounded on both
-        # sides: the GPU step is bit-exact.
+        # Every operation is IEEE-rounded on both sides, and pow rounds as
+        # the host libm does: the GPU step is bit-exact.
         assert exact_fraction(got, ref) == 1.0, f"step {it}: not bit-exact"
 
 
@@ -150,13 +150,13 @@ def test_hllc_known_answers(gpu, oracle):
     assert abs(out[1, 0] - 2.0 / 3.0 * math.sqrt(9.81)) <= 1e-12  # riemann.rs:363-389
 
 
-@pytest.mark.parametrize("pow_mode", ["cr", "libm"])
+@pytest.mark.parametrize("pow_mode", ["libm", "port"])
 @pytest.mark.parametrize("builder", cases.VERIF_CASES, ids=lambda b: b.__name__)
 def test_reference_profiles_on_gpu(gpu, oracle, builder, pow_mode):
     """The reference's verification runs, through the GPU free functions:
-    bitwise against the oracle with the correctly rounded pow, within 1e-10
-    of the oracle with the platform libm pow, and digit for digit against
-    the reference's committed profiles."""
+    bitwise against the oracle with the host libm's pow and with its
+    restatement, and digit for digit against the reference's committed
+    profiles."""
     sim, step = gpu
     oracle.set_pow_mode(pow_mode)
     c = builder()
@@ -176,15 +176,14 @@ def test_reference_profiles_on_gpu(gpu, oracle, builder, pow_mode):
     from tests.test_oracle_golden import run_free_loop
     ref = run_free_loop(oracle, c)
     assert_parity(got, ref)
-    if pow_mode == "cr":
-        assert exact_fraction(got, ref) == 1.0
+    assert exact_fraction(got, ref) == 1.0
     assert np.array_equal(cases.golden_profile(c, got[0]), GOLDEN[c["golden"]])
 
 
-@pytest.mark.parametrize("pow_mode", ["cr", "libm"])
+@pytest.mark.parametrize("pow_mode", ["libm", "port"])
 def test_dam_break_256_simulation(gpu, oracle, pow_mode):
     """Circular dam break 256x256 to t = 10 s through Simulation::run_until:
-    bitwise with the correctly rounded pow, <= 1e-10 with libm's."""
+    bitwise against the oracle with the libm pow and with its restatement."""
     sim, step = gpu
     oracle.set_pow_mode(pow_mode)
     c = cases.dam_break_256()
@@ -199,9 +198,8 @@ def test_dam_break_256_simulation(gpu, oracle, pow_mode):
     assert r["status"] == 0
     assert n_gpu == r["steps"]
     assert_parity(got, (r["h"], r["hu"], r["hv"]))
-    if pow_mode == "cr":
-        assert t_gpu == r["t"]
-        assert exact_fraction(got, (r["h"], r["hu"], r["hv"])) == 1.0
+    assert t_gpu == r["t"]
+    assert exact_fraction(got, (r["h"], r["hu"], r["hv"])) == 1.0
     assert abs(got[0].sum() - c["h"].sum()) <= 1e-10 * c["h"].sum()  # walls conserve mass
 
 

@@ -399,40 +399,61 @@ def test_series_eval(oracle):
     assert oracle.series_eval(t, v, 30.0) == 5.0
 
 
-# ---------------------------------------------------------- correctly rounded pow
-def _cr_pow_reference(x, c):
-    from decimal import Decimal, getcontext
-    getcontext().prec = 70
-    return float(Decimal(float(x)) ** Decimal(float(c)))
+# ------------------------------------------------------ pow as the libm rounds it
+POW_EXPONENTS = (4.0 / 3.0, 3.0 / 5.0, 4.0 / 3.0 - 1.0, 3.0 / 5.0 - 1.0)
 
 
-def test_correctly_rounded_pow(oracle):
-    """hf_pow.h returns the double nearest x^fl(4/3) and x^fl(3/5)
-    (checked against 70-digit decimal arithmetic)."""
-    rng = np.random.default_rng(11)
-    xs = np.concatenate([10.0 ** rng.uniform(-9, 3, 1500), rng.uniform(0.5, 2.0, 500)])
-    for which, c in ((0, 4.0 / 3.0), (1, 3.0 / 5.0)):
-        bad = [x for x in xs if oracle.pow_cr(x, which) != _cr_pow_reference(x, c)]
-        assert not bad, f"misrounded for exponent {c}: {bad[:3]}"
-    assert oracle.pow_cr(0.0, 0) == 0.0 and math.isnan(oracle.pow_cr(-1.0, 0))
-    assert oracle.pow_cr(float("inf"), 0) == float("inf")
+def _pow_samples(rng, n):
+    """Depth-like values (log-uniform 1e-14 .. 1e6), values within 2^-29 of
+    1, and random bit patterns over every positive double (subnormals,
+    the overflow / underflow branches, inf and NaN)."""
+    depth = np.exp(rng.uniform(np.log(1e-14), np.log(1e6), n))
+    near1 = 1.0 + rng.integers(-(1 << 23), 1 << 23, n) * 2.0 ** -52
+    bits = (rng.integers(0, 1 << 63, n, dtype=np.uint64)).view(np.float64)
+    return np.concatenate([depth, near1, np.abs(bits), [0.0, -0.0, 1.0, np.inf, -np.inf,
+                                                        np.nan, -1.0, 5e-324, 1.7e308]])
 
 
-@pytest.mark.parametrize("mode", ["libm", "cr"])
-def test_both_pow_modes_reproduce_reference_profiles(oracle, mode):
-    """The two pow modes differ by at most one rounding per call; both keep
-    every printed digit of the reference's MacDonald run (friction on every
-    cell, Discharge/Depth boundaries)."""
+@pytest.mark.parametrize("y", POW_EXPONENTS)
+def test_pow_restatement_matches_host_libm(oracle, y):
+    """hf_pow.h's pow (what the GPU runs) equals the host C library's pow
+    (what the reference's f64::powf calls) bit for bit: the step's two
+    exponents and the Dual's n - 1, on 3 x 10^6 inputs each."""
+    rng = np.random.default_rng(abs(int(y * 1e6)))
+    n, first = oracle.pow_mismatches(_pow_samples(rng, 1_000_000), y)
+    assert n == 0, f"x^{y!r}: {n} mismatches, e.g. {[float.hex(float(v)) for v in first]}"
+    assert oracle.pow_port(0.0, y) == (0.0 if y > 0 else math.inf)
+    assert math.isnan(oracle.pow_port(-1.0, y)) and oracle.pow_port(1.0, y) == 1.0
+
+
+def test_pow_modes_agree_on_a_wetting_run(oracle):
+    """Whole runs in the oracle's two pow modes (host libm, restatement)
+    are identical bit for bit on a run that wets a dry valley with rain and
+    an inflow (friction on every wet cell, thresholds crossed everywhere),
+    and both keep every printed digit of the reference's MacDonald run."""
     import os
+
+    from hydroflux_b200 import ensemble, workloads
     from tests.test_oracle_golden import run_free_loop
     golden = np.load(os.path.join(os.path.dirname(__file__), "golden", "reference_verif.npz"))
-    oracle.set_pow_mode(mode)
+    s = workloads.valley(n=64, dx=5.0, seed=4, peak=60.0, t_end=600.0)
+    out = {}
     try:
-        c = cases.macdonald()
-        h, _, _ = run_free_loop(oracle, c)
+        for mode in ("libm", "port"):
+            oracle.set_pow_mode(mode)
+            r = oracle.sim_run(s.bed, s.manning, s.dx, s.dy, s.h, s.hu, s.hv,
+                               ensemble.scenario_config(s), s.t_end,
+                               forcing=workloads.oracle_forcing(s))
+            assert r["status"] == 0
+            c = cases.macdonald()
+            h, _, _ = run_free_loop(oracle, c)
+            assert np.array_equal(cases.golden_profile(c, h), golden["macdonald"])
+            out[mode] = r
     finally:
         oracle.set_pow_mode("libm")
-    assert np.array_equal(cases.golden_profile(c, h), golden["macdonald"])
+    assert out["libm"]["steps"] == out["port"]["steps"] > 50
+    for k in ("h", "hu", "hv"):
+        assert np.array_equal(out["libm"][k].view(np.uint64), out["port"][k].view(np.uint64))
 
 
 def test_max_depth_exceeds_relief_flags_a_finite_blow_up(oracle):  # sim.rs:376-386
