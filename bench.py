@@ -17,6 +17,7 @@ use torch.distributed. Rank 0 prints one JSON line.
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import os
 import statistics
@@ -49,13 +50,15 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--workload", default="valley", choices=["valley", "ensemble", "adjoint",
-                                                            "serve", "lanes"],
+                                                            "serve", "lanes", "regimes"],
                    help="valley: the 4096^2 plain step (default line); ensemble: batched "
                         "uneven-size scenarios vs a loop of per-scenario solves; adjoint: "
                         "misfit gradient w.r.t. the Manning field vs the forward solve; "
                         "serve: an arrival stream through the continuous-batching server vs "
                         "a sequential plain solve per request; lanes: zonal Manning "
-                        "derivatives in vector mode vs scalar Dual runs vs the adjoint")
+                        "derivatives in vector mode vs scalar Dual runs vs the adjoint; "
+                        "regimes: the reference's criterion step regimes (all wet, mostly "
+                        "dry) scaled to --n")
     p.add_argument("--calib-n", type=int, default=512, help="adjoint: grid side")
     p.add_argument("--calib-steps", type=int, default=2000, help="adjoint: steps of the misfit")
     p.add_argument("--checkpoint-every", type=int, default=45)
@@ -140,29 +143,30 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def profiled_figure(key):
-    """A per-cell figure of the stage kernel from the committed ncu summary."""
+def profiled_figure(kernel, key):
+    """A per-cell figure of a stage kernel from the committed ncu summary
+    (lines `<kernel>.<key>: value`)."""
     path = os.path.join(ROOT, "profiles", "stage_kernel_traffic.txt")
     try:
         for line in open(path):
-            if line.startswith(key + ":"):
+            if line.startswith(f"{kernel}.{key}:"):
                 return float(line.split(":")[1])
     except OSError:
         pass
     return None
 
 
-def profiled_traffic():
+def profiled_traffic(kernel):
     """DRAM bytes per stage launch per cell from the committed ncu summary."""
-    return profiled_figure("dram_bytes_per_cell_per_launch")
+    return profiled_figure(kernel, "dram_bytes_per_cell_per_launch")
 
 
-def issue_roof(value, clk):
+def issue_roof(kernel, value, clk):
     """The bound the stage kernel actually runs against: instruction issue.
     Warp instructions per cell-update from the committed ncu summary; the
     peak issues one warp instruction per scheduler per cycle (4 per SM) on
     every SM at the SM clock measured during the timed region."""
-    per_cell = profiled_figure("warp_instructions_per_cell_update")
+    per_cell = profiled_figure(kernel, "warp_instructions_per_cell_update")
     if per_cell is None or not clk or not clk.get("sm_mhz"):
         return None
     import torch
@@ -257,7 +261,8 @@ def run_ours(a, d: Dist):
     bytes_per_launch = ALG_BYTES_PER_CELL_UPDATE / STAGE_LAUNCHES_PER_STEP * cells
     achieved_gbs = bytes_per_launch / avg_stage_s / 1e9
     peak, peak_kind = measured_peaks()
-    traffic_per_cell = profiled_traffic()
+    kernel = "k_stage_strip" if sm.stage_kernel() == "strip" else "k_stage_pf"
+    traffic_per_cell = profiled_traffic(kernel)
     sm.close()
 
     # ---- e2e: through the C ABI with host buffers (pinned), copies timed
@@ -322,9 +327,9 @@ def run_ours(a, d: Dist):
         "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
                      "frac": achieved_gbs / peak, "peak_source": peak_kind,
                      "traffic": (traffic_per_cell * cells) if traffic_per_cell else None,
-                     "kernel": "k_stage_pf", "alg_bytes_per_launch": bytes_per_launch,
+                     "kernel": kernel, "alg_bytes_per_launch": bytes_per_launch,
                      "avg_launch_ms": avg_stage_s * 1e3, "launches": stage_launches,
-                     "issue": issue_roof(value / d.world, clk)},
+                     "issue": issue_roof(kernel, value / d.world, clk)},
         "cpu_baseline": cpu,
         "clocks": clk,
     }
@@ -376,6 +381,76 @@ def run_reference(a, d: Dist):
     print(json.dumps(line), flush=True)
 
 
+def run_regimes(a, d: Dist):
+    """The reference's criterion regimes of the step (solver-2d/benches/
+    step.rs:44-75) at --n (default 4096^2): the mostly-dry valley (6.25%
+    wet, where the dry-cell paths dominate) and the all-wet flat bed, each
+    K steps of Simulation::step (SSP-RK2 + Manning, walls) timed with CUDA
+    events; the oracle (1 thread) times one step of each beside it.
+    Replicas on N > 1."""
+    import torch
+
+    from hydroflux_b200 import _lib, abi, workloads
+    from oracle import oracle as O
+    dev = d.local
+    torch.cuda.set_device(dev)
+    _lib.lib()
+    out = {}
+    clocks = ClockSampler(dev)
+    clocks.start()
+    for kind in ("mostly_dry", "all_wet"):
+        scn = workloads.step_regime(kind, a.n)
+        with workloads.simulation_for(scn, device=dev) as sm:
+            h_d, _, _, stream_ptr = sm.device_state()
+            stream = torch.cuda.ExternalStream(stream_ptr, device=dev)
+            sm.run_steps(max(a.warmup, 3))
+            torch.cuda.synchronize(dev)
+            wet = float((h_d > 1e-6).double().mean())
+            d.barrier()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(stream):
+                e0.record(stream)
+            sm.run_steps(a.steps)
+            with torch.cuda.stream(stream):
+                e1.record(stream)
+            torch.cuda.synchronize(dev)
+            ms = d.max(e0.elapsed_time(e1))
+            kernel = sm.stage_kernel()
+            state = sm.states()
+            t0 = sm.time()
+        cpu = None
+        if d.rank == 0 and d.world == 1 and not a.no_cpu_baseline:
+            O.set_threads(1)
+            cfg = abi.make_config(cfl=scn.cfl, boundaries=abi.make_boundaries(*scn.bcs),
+                                  max_dt=scn.max_dt)
+            tc = time.perf_counter()
+            r = O.sim_run(scn.bed, scn.manning, scn.dx, scn.dy, *state, cfg, scn.t_end,
+                          stop_after=1, t0=t0)
+            el = time.perf_counter() - tc
+            assert r["status"] == 0, r["message"]
+            cpu = {"value": scn.n_cells / el, "unit": UNIT, "cores": 1, "kind": "port",
+                   "sample": "1 step of the same state, CPU oracle, 1 thread"}
+        out[kind] = {"value": d.world * scn.n_cells * a.steps / (ms / 1e3), "unit": UNIT,
+                     "ms_per_step": ms / a.steps, "wet_fraction": round(wet, 4),
+                     "stage_kernel": f"k_stage_{kernel}" if kernel == "strip" else "k_stage_pf",
+                     "cpu_baseline": cpu}
+    clk = clocks.stop()
+    line = {"metric": "cell-updates/s (mostly dry)", "value": out["mostly_dry"]["value"],
+            "unit": UNIT, "n_gpus": d.world, "steps": a.steps, "warmup": max(a.warmup, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (the reference's criterion regimes, scaled)",
+            "config": {"workload": f"solver-2d/benches/step.rs regimes at {a.n}x{a.n}, dx 1 m, "
+                                   "SSP-RK2 + Manning 0.03, walls, CFL 0.4",
+                       "l2": "inputs larger than L2" if a.n >= 2048 else "L2-resident",
+                       "parallelism": f"replicas x{d.world}" if d.world > 1 else "single grid"},
+            "regimes": out,
+            "mostly_dry_vs_all_wet": out["mostly_dry"]["value"] / out["all_wet"]["value"],
+            "gpu_launches": 3 * a.steps * 2, "clocks": clk}
+    if d.rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def run_ensemble(a, d: Dist):
     """Batched ensemble (hf_batch_*) against a loop of per-scenario plain GPU
     solves (hf_sim run_steps, one scenario after another), same scenarios and
@@ -392,6 +467,8 @@ def run_ensemble(a, d: Dist):
     allscn = ensemble_scenarios(count=a.scenarios, seed=0)
     mine = [allscn[i] for i in d.shard([s.n_cells for s in allscn])]
     gen_s = time.perf_counter() - t_gen
+    if a.complete:
+        return run_ensemble_complete(a, d, allscn, mine, gen_s)
     cells = np.array([s.n_cells for s in mine], dtype=np.float64)
     ens = Ensemble(mine, device=dev)
     ens.run(max(a.warmup, 3))
@@ -410,14 +487,6 @@ def run_ensemble(a, d: Dist):
     el = d.max(t1 - t0)
     batched = float(np.sum(cells * (st1 - st0)))
     batched_rate = d.sum(batched) / el
-    complete = None
-    if a.complete:
-        t2 = time.perf_counter()
-        left = ens.run()
-        t3 = time.perf_counter()
-        done = sum(1 for k in range(len(mine)) if ens.info(k)["status"] == 0)
-        complete = {"seconds": t3 - t2 + (t1 - t0), "scenarios_completed": done,
-                    "solves_per_s": done / (t3 - t2 + (t1 - t0)), "unfinished": left}
     ens.close()
     # Loop of per-scenario plain solves on a subset, same steps per scenario.
     sub = mine[::max(a.loop_every, 1)]
@@ -446,13 +515,97 @@ def run_ensemble(a, d: Dist):
             "loop_of_plain_solves": {"value": loop_rate, "unit": "cell-updates/s",
                                      "scenarios_timed": len(sub)},
             "speedup_vs_loop": (batched_rate / d.world) / loop_rate if loop_rate else None,
-            "gpu_launches": 4 * a.steps, "generation_s": gen_s, "complete": complete,
+            "gpu_launches": 4 * a.steps, "generation_s": gen_s,
             "schedule": {"chosen": Ensemble.SCHEDULES.get(sched, "untuned"),
                          "tuning_ms_per_candidate": [float(x) for x in tune_ms],
                          "autotune_steps": 64},
             "clocks": clk}
     if d.rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def run_ensemble_complete(a, d: Dist, allscn, mine, gen_s):
+    """Config 3 as its metric states: every scenario solved to its 30-min
+    horizon, batched (one hf_batch handle, run until all have finished)
+    against a loop of plain per-scenario solves (hf_sim run_until, one after
+    another), solves/s of each. The first --scenarios scenarios of the
+    seeded sequence (the same log-uniform side distribution); handle
+    creation and uploads are outside both timings."""
+    import torch
+
+    from hydroflux_b200 import workloads
+    from hydroflux_b200.ensemble import Ensemble
+    dev = d.local
+    # untimed warm-up: one small scenario through each path (module load,
+    # kernel attributes, graph capture)
+    warm = [dataclasses.replace(allscn[0], t_end=30.0)]
+    with Ensemble(warm, device=dev) as e:
+        e.run()
+    with workloads.simulation_for(warm[0], device=dev) as sm:
+        sm.run_until(warm[0].t_end)
+    torch.cuda.synchronize(dev)
+    d.barrier()
+    clocks = ClockSampler(dev)
+    clocks.start()
+    ens = Ensemble(mine, device=dev)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    left = ens.run()
+    torch.cuda.synchronize(dev)
+    batch_s = time.perf_counter() - t0
+    info = [ens.info(k) for k in range(len(mine))]
+    sched, _ = ens.schedule()
+    ens.close()
+    loop_s, loop_steps = [], []
+    for s in mine:
+        with workloads.simulation_for(s, device=dev) as sm:
+            torch.cuda.synchronize(dev)
+            ta = time.perf_counter()
+            sm.run_until(s.t_end)
+            torch.cuda.synchronize(dev)
+            loop_s.append(time.perf_counter() - ta)
+            loop_steps.append(sm.steps())
+    clk = clocks.stop()
+    steps = np.array([x["steps"] for x in info], dtype=np.float64)
+    ok = sum(1 for x in info if x["status"] == 0)
+    cells = np.array([s.n_cells for s in mine], dtype=np.float64)
+    tot = d.gather({"n": len(mine), "ok": ok, "batch_s": batch_s, "loop_s": float(sum(loop_s)),
+                    "cell_updates": float(np.sum(cells * steps)),
+                    "same_steps": bool(np.array_equal(steps, np.array(loop_steps))),
+                    "steps": steps.tolist(), "sides": [s.shape[0] for s in mine],
+                    "loop_each": loop_s})
+    if d.rank != 0:
+        return
+    n_all = sum(x["n"] for x in tot)
+    b_s = max(x["batch_s"] for x in tot)
+    l_s = max(x["loop_s"] for x in tot)
+    st = np.concatenate([np.array(x["steps"]) for x in tot])
+    sides = np.concatenate([np.array(x["sides"]) for x in tot])
+    each = np.concatenate([np.array(x["loop_each"]) for x in tot])
+    small = sides <= 256
+    line = {"metric": "ensemble solves/s to the horizon (batched)", "value": n_all / b_s,
+            "unit": "solves/s", "n_gpus": d.world, "steps": int(st.max()), "warmup": 1,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded valley ensemble)",
+            "config": {"workload": f"the first {a.scenarios} of the seeded 512-scenario ensemble: "
+                                   "side log-uniform in [64, 1024], valley DEM per-scenario "
+                                   "seed, n ~ U[0.02, 0.08], inflow peak 500 x U[0.5, 2] m^3/s, "
+                                   "horizon 30 min each, dx 5 m",
+                       "scenarios": n_all, "cells": int(sum(s.n_cells for s in allscn)),
+                       "parallelism": f"scenarios sharded over {d.world} GPU(s)"},
+            "batched_s": b_s, "scenarios_completed": sum(x["ok"] for x in tot),
+            "unfinished": left,
+            "loop_of_plain_solves": {"value": n_all / l_s, "unit": "solves/s", "seconds": l_s,
+                                     "steps_equal_batched": all(x["same_steps"] for x in tot)},
+            "speedup_vs_loop": l_s / b_s,
+            "cell_updates": sum(x["cell_updates"] for x in tot),
+            "batched_cell_updates_per_s": sum(x["cell_updates"] for x in tot) / b_s,
+            "steps_per_scenario": {"min": int(st.min()), "median": float(np.median(st)),
+                                   "max": int(st.max())},
+            "loop_time_share_sides_le_256": float(each[small].sum() / max(each.sum(), 1e-30)),
+            "schedule": Ensemble.SCHEDULES.get(sched, "untuned"),
+            "generation_s": gen_s, "gpu_launches": None, "clocks": clk}
+    print(json.dumps(line), flush=True)
 
 
 def run_adjoint(a, d: Dist):
@@ -769,6 +922,8 @@ def main():
             run_serve(a, d)
         elif a.workload == "lanes":
             run_lanes(a, d)
+        elif a.workload == "regimes":
+            run_regimes(a, d)
         else:
             run_ours(a, d)
     finally:

@@ -42,6 +42,8 @@ PROTOTYPES = {
     "hf_sim_max_depth_exceeds_relief": (C.c_int, [_VP, C.c_double, C.POINTER(C.c_int)]),
     "hf_sim_set_state_aos": (C.c_int, [_VP, _VP]),
     "hf_sim_set_boundaries": (C.c_int, [_VP, C.POINTER(abi.hf_boundaries)]),
+    "hf_sim_set_stage_kernel": (C.c_int, [_VP, C.c_int]),
+    "hf_sim_stage_kernel": (C.c_int, [_VP, C.POINTER(C.c_int)]),
     "hf_release_cached_memory": (C.c_int, [C.c_int]),
     "hf_sim_error_detail": (C.c_int, [_VP, _D, _D, C.POINTER(C.c_uint64)]),
     "hf_sim_device_state": (C.c_int, [_VP, C.POINTER(_VP), C.POINTER(_VP), C.POINTER(_VP),

@@ -191,9 +191,10 @@ void ForcingHost::release_rain() {
 
 void ForcingHost::release_src() {
   for (void* p : {(void*)d_row, (void*)d_col, (void*)d_off, (void*)d_st, (void*)d_sq,
-                  (void*)d_tile_start, (void*)d_tile_order, (void*)d_dh})
+                  (void*)d_tile_start, (void*)d_tile_order, (void*)d_blk_start,
+                  (void*)d_blk_order, (void*)d_dh})
     dfree(p);
-  d_row = d_col = d_off = d_tile_start = d_tile_order = nullptr;
+  d_row = d_col = d_off = d_tile_start = d_tile_order = d_blk_start = d_blk_order = nullptr;
   d_st = d_sq = d_dh = nullptr;
   n_src = 0;
 }
@@ -211,6 +212,8 @@ ForcingDev ForcingHost::dev() const {
   f.src_q = d_sq;
   f.tile_start = d_tile_start;
   f.tile_order = d_tile_order;
+  f.blk_start = d_blk_start;
+  f.blk_order = d_blk_order;
   f.src_dh = d_dh;
   f.rain_u = rain_u;
   f.src_u = src_u;
@@ -256,13 +259,21 @@ int hf::forcing_set_sources(ForcingHost& f, int64_t nr, int64_t nc, int tiles_x,
     c[k] = (int)cols[k];
   }
   for (int k = 0; k <= ns; ++k) off[k] = (int)offsets[k];
-  // Bucket the sources by stage tile, keeping their order within a tile.
+  // Bucket the sources by stage tile and by strip block, keeping their order
+  // within a bucket (repeated cells accumulate in the caller's order).
+  auto bucket = [&](int nbuckets, auto key, std::vector<int>& start, std::vector<int>& order) {
+    start.assign(nbuckets + 1, 0);
+    order.assign(ns, 0);
+    for (int k = 0; k < ns; ++k) start[key(k) + 1]++;
+    for (int k = 0; k < nbuckets; ++k) start[k + 1] += start[k];
+    std::vector<int> fill(start.begin(), start.end() - 1);
+    for (int k = 0; k < ns; ++k) order[fill[key(k)]++] = k;
+  };
   const int ntiles = tiles_x * tiles_y;
-  std::vector<int> start(ntiles + 1, 0), order(ns);
-  for (int k = 0; k < ns; ++k) start[(r[k] / TY) * tiles_x + c[k] / TX + 1]++;
-  for (int k = 0; k < ntiles; ++k) start[k + 1] += start[k];
-  std::vector<int> fill(start.begin(), start.end() - 1);
-  for (int k = 0; k < ns; ++k) order[fill[(r[k] / TY) * tiles_x + c[k] / TX]++] = k;
+  std::vector<int> start, order, bstart, border;
+  bucket(ntiles, [&](int k) { return (r[k] / TY) * tiles_x + c[k] / TX; }, start, order);
+  const int nb = strip_blocks(nr), nblk = strip_count(nc) * nb;
+  bucket(nblk, [&](int k) { return (c[k] / TX) * nb + r[k] / STRIP_ROWS; }, bstart, border);
   HF_TRY(dalloc(&f.d_row, ns));
   HF_TRY(dalloc(&f.d_col, ns));
   HF_TRY(dalloc(&f.d_off, ns + 1));
@@ -270,6 +281,8 @@ int hf::forcing_set_sources(ForcingHost& f, int64_t nr, int64_t nc, int tiles_x,
   HF_TRY(dalloc(&f.d_sq, npts));
   HF_TRY(dalloc(&f.d_tile_start, ntiles + 1));
   HF_TRY(dalloc(&f.d_tile_order, ns));
+  HF_TRY(dalloc(&f.d_blk_start, nblk + 1));
+  HF_TRY(dalloc(&f.d_blk_order, ns));
   HF_TRY(dalloc(&f.d_dh, ns));
   HF_CUDA(cudaMemcpy(f.d_row, r.data(), ns * sizeof(int), cudaMemcpyHostToDevice));
   HF_CUDA(cudaMemcpy(f.d_col, c.data(), ns * sizeof(int), cudaMemcpyHostToDevice));
@@ -279,6 +292,9 @@ int hf::forcing_set_sources(ForcingHost& f, int64_t nr, int64_t nc, int tiles_x,
   HF_CUDA(cudaMemcpy(f.d_tile_start, start.data(), (ntiles + 1) * sizeof(int),
                      cudaMemcpyHostToDevice));
   HF_CUDA(cudaMemcpy(f.d_tile_order, order.data(), ns * sizeof(int), cudaMemcpyHostToDevice));
+  HF_CUDA(cudaMemcpy(f.d_blk_start, bstart.data(), (nblk + 1) * sizeof(int),
+                     cudaMemcpyHostToDevice));
+  HF_CUDA(cudaMemcpy(f.d_blk_order, border.data(), ns * sizeof(int), cudaMemcpyHostToDevice));
   HF_CUDA(cudaMemset(f.d_dh, 0, ns * sizeof(double)));
   f.n_src = ns;
   return HF_OK;
@@ -299,6 +315,11 @@ struct hf_sim {
   ForcingHost forcing;
   GaugeDev gauge{};  // n == 0: no gauges
   cudaGraphExec_t graphs[3] = {nullptr, nullptr, nullptr};
+  // Stage kernel: HF_STAGE_TILE (k_stage_pf) or HF_STAGE_STRIP (k_stage_strip,
+  // with the TMA descriptors of stage 1's and stage 2's inputs).
+  int stage_kind = HF_STAGE_TILE;
+  int strip_grid = 0;
+  StripMaps maps[2];
   bool cfl_dirty = true;
   double last_dt = 0.0;
   double t = 0.0;
@@ -345,11 +366,42 @@ StageArgs stage_args(const hf_sim* s, bool second) {
   return a;
 }
 
+// One stage of the simulation's step on its stage kernel.
+int launch_sim_stage(hf_sim* s, bool second) {
+  const StageArgs a = stage_args(s, second);
+  if (s->stage_kind == HF_STAGE_STRIP)
+    return launch_stage_strip(a, s->maps[second ? 1 : 0], s->strip_grid, s->stream);
+  return launch_stage(a, s->grid, s->stream);
+}
+
+// Picks the stage kernel: the strip kernel where it is asked for (or, for
+// `kind` auto, where the grid has enough strip blocks per CTA) and its TMA
+// descriptors can be made, else the tile kernel.
+int choose_stage_kernel(hf_sim* s, int kind) {
+  s->stage_kind = HF_STAGE_TILE;
+  if (kind == HF_STAGE_TILE) return HF_OK;
+  int g = strip_grid_size(s->nr, s->nc, s->device);
+  if (g == 0 && kind == HF_STAGE_STRIP) {  // forced on a small grid: one CTA per block at most
+    g = strip_grid_size(1 << 20, 1 << 12, s->device);
+    const long long nq = (long long)strip_count(s->nc) * strip_blocks(s->nr);
+    if (nq < g) g = (int)nq;
+  }
+  if (g > 0 && strip_maps(stage_args(s, false), s->maps[0]) &&
+      strip_maps(stage_args(s, true), s->maps[1])) {
+    s->stage_kind = HF_STAGE_STRIP;
+    s->strip_grid = g;
+  } else if (kind == HF_STAGE_STRIP) {
+    return fail(HF_ERR_UNSUPPORTED,
+                "the strip stage kernel needs an even column count and 16-byte aligned fields");
+  }
+  return HF_OK;
+}
+
 int enqueue_step(hf_sim* s) {
   HF_TRY(launch_control(s->d_ctrl, s->dx, s->dy, s->forcing.dev(), s->stream));
-  HF_TRY(launch_stage(stage_args(s, false), s->grid, s->stream));
+  HF_TRY(launch_sim_stage(s, false));
   if (s->cfg.integrator == HF_SSPRK2)
-    HF_TRY(launch_stage(stage_args(s, true), s->grid, s->stream));
+    HF_TRY(launch_sim_stage(s, true));
   else
     HF_TRY(launch_finalize(stage_args(s, true), s->grid, s->stream));
   if (s->gauge.n > 0) HF_TRY(launch_gauges(s->d_ctrl, s->d_h, s->gauge, 0, s->stream));
@@ -581,6 +633,7 @@ int hf_sim_create(const hf_mesh_desc* mesh, const double* h, const double* hu, c
       return done(cuda_fail(failed_call_error(), "init ctrl"));
   }
   if ((rc = upload3(s, h, hu, hv)) != HF_OK) return done(rc);
+  if ((rc = choose_stage_kernel(s, HF_STAGE_AUTO)) != HF_OK) return done(rc);
   *out = s;
   return HF_OK;
 }
@@ -689,11 +742,10 @@ int hf_sim_run_steps_timed(hf_sim* s, uint64_t n_steps, double t_target, double*
     rc = launch_control(s->d_ctrl, s->dx, s->dy, s->forcing.dev(), s->stream);
     if (rc) break;
     cudaEventRecord(ev[3 * k], s->stream);
-    rc = launch_stage(stage_args(s, false), s->grid, s->stream);
+    rc = launch_sim_stage(s, false);
     if (rc) break;
     cudaEventRecord(ev[3 * k + 1], s->stream);
-    rc = ssp ? launch_stage(stage_args(s, true), s->grid, s->stream)
-             : launch_finalize(stage_args(s, true), s->grid, s->stream);
+    rc = ssp ? launch_sim_stage(s, true) : launch_finalize(stage_args(s, true), s->grid, s->stream);
     cudaEventRecord(ev[3 * k + 2], s->stream);
     if (rc == HF_OK && s->gauge.n > 0)
       rc = launch_gauges(s->d_ctrl, s->d_h, s->gauge, 0, s->stream);
@@ -796,6 +848,22 @@ int hf_sim_set_boundaries(hf_sim* s, const hf_boundaries* bcs) {
   s->cfg.boundaries = *bcs;
   drop_graphs(s);
   s->cfl_dirty = true;  // ghost wave speeds depend on the boundaries
+  return HF_OK;
+}
+
+int hf_sim_set_stage_kernel(hf_sim* s, int kind) {
+  if (!s) return fail(HF_ERR_INVALID_ARG, "null handle");
+  if (kind != HF_STAGE_AUTO && kind != HF_STAGE_TILE && kind != HF_STAGE_STRIP)
+    return fail(HF_ERR_INVALID_ARG, "unknown stage kernel");
+  DeviceGuard guard(s->device);
+  cudaStreamSynchronize(s->stream);
+  drop_graphs(s);
+  return choose_stage_kernel(s, kind);
+}
+
+int hf_sim_stage_kernel(const hf_sim* s, int* kind) {
+  if (!s || !kind) return fail(HF_ERR_INVALID_ARG, "null argument");
+  *kind = s->stage_kind;
   return HF_OK;
 }
 

@@ -1,6 +1,8 @@
 // hf_internal.h -- structures shared by the kernels and the C-ABI layer.
 #pragma once
 
+#include <cuda.h>  // CUtensorMap (types only; the driver is reached through the runtime)
+
 #include <cstdint>
 #include <cstring>
 
@@ -33,6 +35,14 @@ constexpr int NTHREADS = HF_THREADS;
 constexpr int ROWS_PER_PASS = NTHREADS / TX;           // tile rows one pass of the CTA covers
 constexpr int CELLS_PER_THREAD = TX * TY / NTHREADS;   // cells a thread updates per tile
 static_assert(NTHREADS % TX == 0 && TY % ROWS_PER_PASS == 0, "tile / thread shape");
+
+// Strip geometry of the streaming stage kernel (hf_strip.cuh): a CTA walks
+// down a TX-wide column of blocks of STRIP_ROWS rows, carrying the halo rows
+// of one block into the next. Blocks are numbered strip-major:
+// q = (column / TX) * strip_blocks(nr) + row / STRIP_ROWS.
+constexpr int STRIP_ROWS = 7;
+HF_ARITH_HD int strip_blocks(int64_t nr) { return (int)((nr + STRIP_ROWS - 1) / STRIP_ROWS); }
+HF_ARITH_HD int strip_count(int64_t nc) { return (int)((nc + TX - 1) / TX); }
 
 // Boundary descriptor in kernel arguments; sides in Boundaries2D order.
 struct BcDev {
@@ -99,6 +109,10 @@ struct ForcingDev {
   const double* src_q;
   const int* tile_start;
   const int* tile_order;
+  // The same sources bucketed by strip block (blk_start has one entry per
+  // strip block + 1).
+  const int* blk_start;
+  const int* blk_order;
   double* src_dh;  // per source, set each step by the control kernel
   // Series units: a series is sampled at t / t_div and its value converted
   // as (v * v_mul) / v_div (identity by default; see hf_sim_set_rain_units).
@@ -204,6 +218,22 @@ int launch_hllc(int x_dir, int64_t n, const double* ul, const double* ur, double
                 void* stream);
 int stage_grid_size(int tiles, int device);
 size_t stage_smem_bytes();
+
+// TMA descriptors of one stage's inputs for the strip kernel (hf_strip.cuh):
+// depth rows (box 40 x (STRIP_ROWS + 1)), bed, hu, hv (40 x STRIP_ROWS).
+struct StripMaps {
+  CUtensorMap h, z, hu, hv;
+};
+// Encodes the descriptors of a stage's inputs (a.in_h, a.z, a.in_hu,
+// a.in_hv); false when the grid cannot be fetched that way (an odd column
+// count gives rows that do not start on 16 bytes; an unaligned buffer; no
+// driver entry point), in which case the tile kernel runs.
+bool strip_maps(const StageArgs& a, StripMaps& m);
+// CTAs of the strip kernel for an nr x nc grid on `device` (also raises its
+// shared-memory limit; never inside a stream capture); 0 when the grid has
+// too few strip blocks per CTA for streaming to pay.
+int strip_grid_size(int64_t nr, int64_t nc, int device);
+int launch_stage_strip(const StageArgs& a, const StripMaps& m, int grid, void* stream);
 // DualD tangent stage / finalize (same arguments; tangent arrays in a.tan).
 int stage_dual_grid_size(int tiles, int device);
 // lanes > 1 (vector mode): one grid of `grid` CTAs per tangent lane
@@ -276,6 +306,8 @@ struct ForcingHost {
   double* d_sq = nullptr;
   int* d_tile_start = nullptr;
   int* d_tile_order = nullptr;
+  int* d_blk_start = nullptr;
+  int* d_blk_order = nullptr;
   double* d_dh = nullptr;
   SeriesUnits rain_u, src_u;
   void release_rain();

@@ -22,6 +22,7 @@
 #include "hf_device.cuh"
 #include "hf_internal.h"
 #include "hf_stage.cuh"
+#include "hf_strip.cuh"
 
 namespace hf {
 
@@ -109,6 +110,64 @@ __global__ void __launch_bounds__(NTHREADS, HF_MIN_BLOCKS) k_stage_pf(const Stag
       stage_tile<double, true, true>(A, P.s, tile, sxm, sym, nonfin, P.hst, next);
     else
       stage_tile<double, true>(A, P.s, tile, sxm, sym, nonfin, P.hst, next);
+  }
+  if (A.finalize) {
+    block_reduce_speeds(sxm, sym, nonfin, A.ctrl);
+    if (blockIdx.x == 0 && threadIdx.x == 0) commit_clock(A.ctrl);
+  }
+}
+
+// The f64 stage of one grid as a streaming walk down 32-column strips in
+// blocks of STRIP_ROWS rows (hf_strip.cuh): each CTA takes a contiguous
+// range of the strip-major block sequence, computes only the rows a block
+// adds to the previous one, and fetches the next block's new input rows with
+// TMA while it computes. Results are those of k_stage_pf.
+__global__ void __launch_bounds__(NTHREADS, HF_MIN_BLOCKS)
+    k_stage_strip(const StageArgs A, const __grid_constant__ StripMaps M) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  StripSmem& S = *reinterpret_cast<StripSmem*>(
+      smem_raw + ((128 - (smem_addr(smem_raw) & 127)) & 127));
+  if (!A.ctrl->active) return;
+  const int nb = strip_blocks(A.nr);
+  const long long nq = (long long)strip_count(A.nc) * nb;
+  long long q = nq * blockIdx.x / gridDim.x;
+  const long long q_end = nq * (blockIdx.x + 1) / gridDim.x;
+  const double dt = A.ctrl->dt;
+  const double dt_dx = dt / A.dx;  // update.rs:930-931
+  const double dt_dy = dt / A.dy;
+  double sxm = 0.0, sym = 0.0;
+  unsigned long long nonfin = 0;
+  if (threadIdx.x == 0) mbar_init(&S.mbar);
+  __syncthreads();
+  unsigned parity = 0;
+  bool cold = true;
+  while (q < q_end) {
+    const int strip = (int)(q / nb), b = (int)(q - (long long)strip * nb);
+    const int gi0 = b * SR, gj0 = strip * TX;
+    const bool in = interior_block(A, gi0, gj0);
+    const bool next_warm = q + 1 < q_end && b + 1 < nb;
+    if (cold) {
+      if (next_warm && threadIdx.x == 0) strip_fetch(S, M, gi0 + SR, gj0);
+      if (in) strip_cold<true>(A, S, gi0, gj0); else strip_cold<false>(A, S, gi0, gj0);
+    }
+    if (next_warm) {
+      if (!strip_wait(S, parity, A.ctrl)) return;
+      parity ^= 1;
+    }
+    if (in) strip_alpha_prims<true>(A, S, gi0, gj0, cold ? -1 : 1, next_warm, dt_dx, dt_dy);
+    else strip_alpha_prims<false>(A, S, gi0, gj0, cold ? -1 : 1, next_warm, dt_dx, dt_dy);
+    __syncthreads();
+    if (in) strip_update<true>(A, S, gi0, gj0, q, dt, dt_dx, dt_dy, sxm, sym, nonfin);
+    else strip_update<false>(A, S, gi0, gj0, q, dt, dt_dx, dt_dy, sxm, sym, nonfin);
+    __syncthreads();
+    ++q;
+    cold = !next_warm;
+    if (cold) continue;
+    strip_shift(S);
+    __syncthreads();
+    if (q + 1 < q_end && b + 2 < nb && threadIdx.x == 0) strip_fetch(S, M, gi0 + 2 * SR, gj0);
+    if (interior_block(A, gi0 + SR, gj0)) strip_new_rows<true>(A, S, gi0 + SR, gj0);
+    else strip_new_rows<false>(A, S, gi0 + SR, gj0);
   }
   if (A.finalize) {
     block_reduce_speeds(sxm, sym, nonfin, A.ctrl);
@@ -217,7 +276,7 @@ __device__ void finalize_tiles(const StageArgs& A, Ctrl* ctrl, double& sxm, doub
       T h = Field<T>::ld(A.in_h, A.tan.in_h, g);
       T hu = Field<T>::ld(A.in_hu, A.tan.in_hu, g);
       T hv = Field<T>::ld(A.in_hv, A.tan.in_hv, g);
-      finalize_cell<T>(A, ctrl, dt, gi, gj, g, src_lo, src_hi, h, hu, hv);
+      finalize_cell<T>(A, ctrl, dt, gi, gj, g, A.f.tile_order, src_lo, src_hi, h, hu, hv);
       cfl_cell(A, gi, gj, g, val(h), val(hu), val(hv), sxm, sym);
       if (ctrl->check_finite && !isfinite(val(h))) ++nonfin;
       Field<T>::st(A.out_h, A.tan.out_h, g, h);
@@ -610,6 +669,76 @@ int stage_grid_size(int tiles, int device) {
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   int g = per_sm * (sms > 0 ? sms : 148);
   return tiles < g ? (tiles < 1 ? 1 : tiles) : g;
+}
+
+// ---- strip kernel: descriptors, grid size, launch
+namespace {
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                 const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                 const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                 CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiled encode_tiled() {
+  static EncodeTiled fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      p = nullptr;
+    }
+    return reinterpret_cast<EncodeTiled>(p);
+  }();
+  return fn;
+}
+// An nr x nc row-major f64 array, boxes of 40 columns x `rows` rows; cells
+// outside the array read as zeros.
+bool encode_rows(CUtensorMap& m, const double* base, int64_t nr, int64_t nc, int rows) {
+  EncodeTiled enc = encode_tiled();
+  if (!enc || !base || ((uintptr_t)base & 15) || (nc * sizeof(double)) % 16) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)nc, (cuuint64_t)nr};
+  const cuuint64_t strides[1] = {(cuuint64_t)nc * sizeof(double)};
+  const cuuint32_t box[2] = {40u, (cuuint32_t)rows};
+  const cuuint32_t estr[2] = {1u, 1u};
+  return enc(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(base), dims, strides,
+             box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+         CUDA_SUCCESS;
+}
+constexpr size_t kStripSmemBytes = sizeof(StripSmem) + 128;  // + alignment of the base
+}  // namespace
+
+bool strip_maps(const StageArgs& a, StripMaps& m) {
+  return encode_rows(m.h, a.in_h, a.nr, a.nc, STRIP_ROWS + 1) &&
+         encode_rows(m.z, a.z, a.nr, a.nc, STRIP_ROWS) &&
+         encode_rows(m.hu, a.in_hu, a.nr, a.nc, STRIP_ROWS) &&
+         encode_rows(m.hv, a.in_hv, a.nr, a.nc, STRIP_ROWS);
+}
+
+int strip_grid_size(int64_t nr, int64_t nc, int device) {
+  static int cached[64] = {0};
+  int per_sm = 0, sms = 0;
+  if (device >= 0 && device < 64 && cached[device] > 0) {
+    per_sm = cached[device];
+  } else {
+    DevGuard dg(device);
+    cudaFuncSetAttribute(k_stage_strip, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)kStripSmemBytes);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stage_strip, NTHREADS,
+                                                  kStripSmemBytes);
+    cudaGetLastError();
+    if (per_sm < 1) return 0;
+    if (device >= 0 && device < 64) cached[device] = per_sm;
+  }
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  const long long g = (long long)per_sm * (sms > 0 ? sms : 148);
+  const long long nq = (long long)strip_count(nc) * strip_blocks(nr);
+  return nq >= 4 * g ? (int)g : 0;
+}
+
+int launch_stage_strip(const StageArgs& a, const StripMaps& m, int grid, void* stream) {
+  k_stage_strip<<<grid, NTHREADS, kStripSmemBytes, (cudaStream_t)stream>>>(a, m);
+  return cuda_rc(cudaGetLastError());
 }
 
 int stage_dual_grid_size(int tiles, int device) {

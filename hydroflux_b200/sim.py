@@ -345,6 +345,18 @@ class Simulation:
         raise_for(lib().hf_sim_get_state(self._h, h.ctypes.data, hu.ctypes.data, hv.ctypes.data))
         return h, hu, hv
 
+    STAGE_KERNELS = {"auto": 0, "tile": 1, "strip": 2}
+
+    def set_stage_kernel(self, kind: str) -> None:
+        """'tile', 'strip' or 'auto' (hf_sim_set_stage_kernel): which kernel
+        runs the stages; results are bit-identical."""
+        raise_for(lib().hf_sim_set_stage_kernel(self._h, self.STAGE_KERNELS[kind]))
+
+    def stage_kernel(self) -> str:
+        k = C.c_int()
+        raise_for(lib().hf_sim_stage_kernel(self._h, C.byref(k)))
+        return {v: n for n, v in self.STAGE_KERNELS.items()}[k.value]
+
     def max_depth_exceeds_relief(self, factor: float) -> bool:
         """max_depth_exceeds_relief(sim.states(), sim.mesh(), factor)
         (sim.rs:248-271): whether the largest depth exceeds `factor` times

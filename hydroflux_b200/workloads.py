@@ -204,6 +204,32 @@ def calibration_problem(n: int = 512, dx: float = 5.0, seed: int = 0, n_steps: i
     return CalibrationProblem(s, int(n_steps), gauges, hidden)
 
 
+def step_regime(kind: str, n: int = 4096) -> Scenario:
+    """The reference's two criterion regimes of the step
+    (solver-2d/benches/step.rs:44-75), on an n x n grid of 1 m cells, Manning
+    0.03, walls, CFL 0.4, no forcing. The reference runs them at 256 x 256;
+    here the mostly-dry valley keeps its wet fraction at any n (the water
+    level scales with n / 256, so the wet channel stays 1/16 of the width).
+
+    all_wet: flat bed, h = 1 + 0.2 i/n + 0.1 j/n, hu = 0.1 h, hv = 0.05 h.
+    mostly_dry: bed 0.05 |j - n/2|, level 0.4 n/256, h = max(level - z, 0),
+    hu = 0, hv = 0.1 h (6.25% of the cells wet, in one channel strip)."""
+    i = np.arange(n, dtype=np.float64)[:, None]
+    j = np.arange(n, dtype=np.float64)[None, :]
+    if kind == "all_wet":
+        bed = np.zeros((n, n))
+        h = 1.0 + 0.2 * (i / n) + 0.1 * (j / n)
+        hu, hv = 0.1 * h, 0.05 * h
+    elif kind == "mostly_dry":
+        bed = np.broadcast_to(0.05 * np.abs(j - n / 2.0), (n, n)).copy()
+        h = np.maximum(0.4 * n / 256.0 - bed, 0.0)
+        hu, hv = np.zeros((n, n)), 0.1 * h
+    else:
+        raise ValueError(f"unknown regime {kind!r}")
+    return Scenario(kind, bed, np.full((n, n), 0.03), 1.0, 1.0, h, hu, hv,
+                    bcs=((1, 0.0),) * 4, cfl=0.4, t_end=float("inf"), max_dt=60.0)
+
+
 def simulation_for(s: Scenario, device: int = 0, integrator=None):
     """A hydroflux_b200.sim.Simulation set up with the scenario's forcings."""
     from . import sim as S

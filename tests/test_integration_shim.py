@@ -1,11 +1,12 @@
-"""The Rust shim of the integration guide against include/hydroflux_gpu.h.
+"""The Rust FFI module include/hydroflux_gpu.rs against include/hydroflux_gpu.h.
 
-The guide writes out, in its ```rust blocks, the FFI declarations a
-maintainer would paste into the crate. There is no Rust toolchain here, so
-that shim is not compiled. This test stands in for the compile-time half of
-that: every `extern "C"` function of the shim must exist in the header with
-the same return and parameter types, and every `#[repr(C)]` struct must list
-the header struct's fields in the same order with the same types."""
+The .rs file holds the FFI declarations a maintainer adds to the Rust crate
+to call this library. There is no Rust toolchain here, so it is not
+compiled. This test stands in for the compile-time half of that: every C
+function of the header is declared in the module, every `extern "C"`
+function of the module exists in the header with the same return and
+parameter types, and every `#[repr(C)]` struct lists the header struct's
+fields in the same order with the same types."""
 import os
 import re
 
@@ -13,7 +14,7 @@ import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 HEADER = os.path.join(ROOT, "include", "hydroflux_gpu.h")
-DOC = os.path.join(ROOT, "INTEGRATION.md")
+RUST = os.path.join(ROOT, "include", "hydroflux_gpu.rs")
 
 RUST_SCALARS = {"f64": "double", "i64": "int64_t", "u64": "uint64_t", "i32": "int32_t",
                 "c_int": "int", "c_char": "char", "c_void": "void"}
@@ -74,14 +75,9 @@ def header():
     return structs, funcs
 
 
-def rust_blocks():
-    text = open(DOC).read()
-    return re.findall(r"```rust\n(.*?)```", text, flags=re.S)
-
-
 def shim():
     structs, funcs = {}, {}
-    for block in rust_blocks():
+    for block in [open(RUST).read()]:
         code = re.sub(r"//[^\n]*", " ", block)
         for m in re.finditer(r"#\[repr\(C\)\](?:\s*#\[derive\([^)]*\)\])?\s*pub struct (\w+)\s*\{(.*?)\}",
                              code, flags=re.S):
@@ -107,8 +103,15 @@ def shim():
 def test_parsers_see_the_shim():
     s_structs, s_funcs = shim()
     h_structs, h_funcs = header()
-    assert len(s_funcs) >= 20 and len(s_structs) >= 5
+    assert len(s_funcs) >= 60 and len(s_structs) >= 7
     assert "hf_sim_create_aos" in h_funcs and "hf_config" in h_structs
+
+
+def test_module_declares_every_header_function_and_struct():
+    s_structs, s_funcs = shim()
+    h_structs, h_funcs = header()
+    assert sorted(h_funcs) == sorted(s_funcs)
+    assert sorted(h_structs) == sorted(rust_type(r) for r in s_structs)
 
 
 def test_shim_functions_match_the_header():
