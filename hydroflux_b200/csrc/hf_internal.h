@@ -86,6 +86,12 @@ struct Ctrl {
   // max_depth_exceeds_relief accumulators (order-preserving keys of doubles):
   // max depth (from 0), max bed, min bed.
   unsigned long long relief_keys[3];
+  // Strip stage kernel: block counters of the dynamic schedule of stage 1 /
+  // stage 2, and the blocks its stages skipped as dry in the current and the
+  // previous step (which picks the schedule). The control kernel rolls them
+  // over at the start of every step.
+  unsigned long long strip_claim[2];
+  unsigned long long strip_dry, strip_dry_last;
 };
 
 struct SeriesUnits {

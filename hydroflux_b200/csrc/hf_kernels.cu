@@ -118,28 +118,23 @@ __global__ void __launch_bounds__(NTHREADS, HF_MIN_BLOCKS) k_stage_pf(const Stag
 }
 
 // The f64 stage of one grid as a streaming walk down 32-column strips in
-// blocks of STRIP_ROWS rows (hf_strip.cuh): each CTA takes a contiguous
-// range of the strip-major block sequence, computes only the rows a block
-// adds to the previous one, and fetches the next block's new input rows with
-// TMA while it computes. Results are those of k_stage_pf.
-__global__ void __launch_bounds__(NTHREADS, HF_MIN_BLOCKS)
-    k_stage_strip(const StageArgs A, const __grid_constant__ StripMaps M) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  StripSmem& S = *reinterpret_cast<StripSmem*>(
-      smem_raw + ((128 - (smem_addr(smem_raw) & 127)) & 127));
-  if (!A.ctrl->active) return;
-  const int nb = strip_blocks(A.nr);
-  const long long nq = (long long)strip_count(A.nc) * nb;
-  long long q = nq * blockIdx.x / gridDim.x;
-  const long long q_end = nq * (blockIdx.x + 1) / gridDim.x;
-  const double dt = A.ctrl->dt;
-  const double dt_dx = dt / A.dx;  // update.rs:930-931
-  const double dt_dy = dt / A.dy;
-  double sxm = 0.0, sym = 0.0;
-  unsigned long long nonfin = 0;
-  if (threadIdx.x == 0) mbar_init(&S.mbar);
-  __syncthreads();
-  unsigned parity = 0;
+// blocks of STRIP_ROWS rows (hf_strip.cuh): a CTA takes a contiguous range
+// of the strip-major block sequence, computes only the rows a block adds to
+// the previous one, and fetches the next block's new input rows with TMA
+// while it computes. Results are those of k_stage_pf.
+//
+// Schedule: while the grid is mostly wet, each CTA takes one equal range
+// (no atomics, one cold block per range). When the previous step skipped
+// more than 1/16 of the blocks as dry, the cost of a block depends on where
+// the water is, so CTAs claim ranges of STRIP_CHUNK blocks from a counter
+// instead. Either way every block is computed once, the same way.
+constexpr int STRIP_CHUNK = 16;
+
+__device__ __forceinline__ bool strip_range(const StageArgs& A, const StripMaps& M,
+                                            StripSmem& S, long long q, long long q_end, int nb,
+                                            unsigned& parity, double dt, double dt_dx,
+                                            double dt_dy, double& sxm, double& sym,
+                                            unsigned long long& nonfin) {
   bool cold = true;
   while (q < q_end) {
     const int strip = (int)(q / nb), b = (int)(q - (long long)strip * nb);
@@ -151,7 +146,7 @@ __global__ void __launch_bounds__(NTHREADS, HF_MIN_BLOCKS)
       if (in) strip_cold<true>(A, S, gi0, gj0); else strip_cold<false>(A, S, gi0, gj0);
     }
     if (next_warm) {
-      if (!strip_wait(S, parity, A.ctrl)) return;
+      if (!strip_wait(S, parity, A.ctrl)) return false;
       parity ^= 1;
     }
     if (in) strip_alpha_prims<true>(A, S, gi0, gj0, cold ? -1 : 1, next_warm, dt_dx, dt_dy);
@@ -169,9 +164,48 @@ __global__ void __launch_bounds__(NTHREADS, HF_MIN_BLOCKS)
     if (interior_block(A, gi0 + SR, gj0)) strip_new_rows<true>(A, S, gi0 + SR, gj0);
     else strip_new_rows<false>(A, S, gi0 + SR, gj0);
   }
+  return true;
+}
+
+__global__ void __launch_bounds__(NTHREADS, HF_MIN_BLOCKS)
+    k_stage_strip(const StageArgs A, const __grid_constant__ StripMaps M) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  StripSmem& S = *reinterpret_cast<StripSmem*>(
+      smem_raw + ((128 - (smem_addr(smem_raw) & 127)) & 127));
+  __shared__ long long s_claim;
+  Ctrl* ctrl = A.ctrl;
+  if (!ctrl->active) return;
+  const int nb = strip_blocks(A.nr);
+  const long long nq = (long long)strip_count(A.nc) * nb;
+  const double dt = ctrl->dt;
+  const double dt_dx = dt / A.dx;  // update.rs:930-931
+  const double dt_dy = dt / A.dy;
+  double sxm = 0.0, sym = 0.0;
+  unsigned long long nonfin = 0;
+  if (threadIdx.x == 0) mbar_init(&S.mbar);
+  __syncthreads();
+  unsigned parity = 0;
+  const bool dynamic = 16ull * ctrl->strip_dry_last > 2ull * (unsigned long long)nq;
+  unsigned long long* counter = &ctrl->strip_claim[A.finalize ? 1 : 0];
+  for (int round = 0;; ++round) {
+    long long q0, q1;
+    if (!dynamic) {
+      if (round > 0) break;
+      q0 = nq * blockIdx.x / gridDim.x;
+      q1 = nq * (blockIdx.x + 1) / gridDim.x;
+    } else {
+      if (threadIdx.x == 0) s_claim = (long long)atomicAdd(counter, (unsigned long long)STRIP_CHUNK);
+      __syncthreads();
+      q0 = s_claim;
+      __syncthreads();  // s_claim is read before the next claim overwrites it
+      if (q0 >= nq) break;
+      q1 = q0 + STRIP_CHUNK < nq ? q0 + STRIP_CHUNK : nq;
+    }
+    if (!strip_range(A, M, S, q0, q1, nb, parity, dt, dt_dx, dt_dy, sxm, sym, nonfin)) return;
+  }
   if (A.finalize) {
-    block_reduce_speeds(sxm, sym, nonfin, A.ctrl);
-    if (blockIdx.x == 0 && threadIdx.x == 0) commit_clock(A.ctrl);
+    block_reduce_speeds(sxm, sym, nonfin, ctrl);
+    if (blockIdx.x == 0 && threadIdx.x == 0) commit_clock(ctrl);
   }
 }
 
@@ -409,7 +443,12 @@ __device__ __forceinline__ void source_increment(const Ctrl* c, double dx, doubl
 
 __global__ void k_control(Ctrl* c, double dx, double dy, ForcingDev f) {
   __shared__ int s_go;
-  if (threadIdx.x == 0) s_go = control_step(c, dx, dy, f);
+  if (threadIdx.x == 0) {
+    c->strip_dry_last = c->strip_dry;
+    c->strip_dry = 0;
+    c->strip_claim[0] = c->strip_claim[1] = 0;
+    s_go = control_step(c, dx, dy, f);
+  }
   __syncthreads();
   if (s_go)
     for (int k = threadIdx.x; k < f.n_src; k += blockDim.x) source_increment(c, dx, dy, f, k);

@@ -16,10 +16,13 @@
 // (cp.async.bulk.tensor, no multicast) into staging buffers while the
 // current block computes; completion is an mbarrier with a bounded wait.
 //
-// Work is split statically: the strip-major sequence of blocks (q = strip *
-// blocks_per_strip + block) is cut into one contiguous range per CTA, so a
-// CTA starts from scratch (a "cold" block, as k_stage_pf does for a tile)
-// only at the start of its range and where the range enters a new strip.
+// Work is split into contiguous ranges of the strip-major sequence of blocks
+// (q = strip * blocks_per_strip + block): one equal range per CTA while the
+// grid is wet, ranges of 16 blocks claimed from a counter once many blocks
+// are dry (k_stage_strip). A CTA starts from scratch (a "cold" block, as
+// k_stage_pf does for a tile) only at the start of a range and where the
+// range enters a new strip. Interior blocks whose depths are all at or
+// below H_DRY write their zero slopes and faces instead of computing them.
 //
 // Every cell is computed by the same item functions as k_stage_pf's
 // (slope_at, face_at, alpha_at, update_at in hf_stage.cuh), on the same
@@ -122,6 +125,30 @@ __device__ __forceinline__ bool interior_block(const StageArgs& A, int gi0, int 
   return gi0 >= 4 && gj0 >= 4 && gi0 + SR + 4 <= A.nr && gj0 + TX + 4 <= A.nc;
 }
 
+// Dry blocks. When every depth a block's slopes and faces read is at or
+// below H_DRY and the block reaches no side, every slope is the limiter's
+// zero (a dry cell within two cells, update.rs:459-540) and every face is a
+// dry-dry face with zero flux (update.rs:890-926): the block writes those
+// zeros instead of computing them, and its cells then take the isolated-dry
+// update. Votes over the depth buffer entries [k0, k1) (with a barrier);
+// a dry block is counted for the schedule of the next step.
+__device__ __forceinline__ bool strip_all_dry(StripSmem& S, int k0, int k1, Ctrl* ctrl) {
+  bool dry = true;
+  for (int k = k0 + threadIdx.x; k < k1; k += NTHREADS) dry &= S.h[k] <= H_DRY;
+  const bool all = __syncthreads_and(dry);
+  if (all && threadIdx.x == 0) atomicAdd(&ctrl->strip_dry, 1ull);
+  return all;
+}
+__device__ __forceinline__ void zero_rows(double* a, double* b, double* c, int k0, int k1) {
+  for (int k = k0 + threadIdx.x; k < k1; k += NTHREADS) a[k] = b[k] = c[k] = 0.0;
+}
+__device__ __forceinline__ void zero_faces(StripSmem& S, int x0, int x1, int y0, int y1) {
+  for (int k = x0 + threadIdx.x; k < x1; k += NTHREADS)
+    S.fxm[k] = S.fxnm[k] = S.fxnp[k] = S.fxt[k] = 0.0;
+  for (int k = y0 + threadIdx.x; k < y1; k += NTHREADS)
+    S.fym[k] = S.fynm[k] = S.fynp[k] = S.fyt[k] = 0.0;
+}
+
 // A block from scratch: inputs (plain loads, zeros outside the grid),
 // primitives, slopes and faces of every row of its buffers.
 template <bool IN>
@@ -152,7 +179,17 @@ __device__ void strip_cold(const StageArgs& A, StripSmem& S, int gi0, int gj0) {
       S.v[k3] = vv;
     }
   }
-  __syncthreads();
+  if constexpr (IN) {  // the vote is also the barrier after the loads
+    if (strip_all_dry(S, 0, SH4 * R4W, A.ctrl)) {
+      zero_rows(S.sxe, S.sxu, S.sxv, 0, SHX * SXW);
+      zero_rows(S.sye, S.syu, S.syv, 0, SHY * SYW);
+      zero_faces(S, 0, SHFX * FXW, 0, SHFY * FYW);
+      __syncthreads();
+      return;
+    }
+  } else {
+    __syncthreads();
+  }
   for (int k = tid; k < SHX * SXW + SHY * SYW; k += NTHREADS) {
     if (k < SHX * SXW) {
       const int r = k / SXW;
@@ -252,6 +289,16 @@ template <bool IN>
 __device__ __forceinline__ void strip_new_rows(const StageArgs& A, StripSmem& S, int gi0,
                                                int gj0) {
   constexpr int NX = SR * SXW, NY = SR * SYW;
+  // new slopes and faces read the depths of rows [0, SR + 4)
+  if constexpr (IN) {
+    if (strip_all_dry(S, 4 * R4W, SH4 * R4W, A.ctrl)) {
+      zero_rows(S.sxe, S.sxu, S.sxv, isx(1, -2), isx(SR + 1, -2));
+      zero_rows(S.sye, S.syu, S.syv, isy(2, -1), isy(SR + 2, -1));
+      zero_faces(S, ifx(1, -1), ifx(SR + 1, -1), ify(2, -1), ify(SR + 2, -1));
+      __syncthreads();
+      return;
+    }
+  }
   for (int k = threadIdx.x; k < NX + NY; k += NTHREADS) {
     if (k < NX) {
       const int r = k / SXW;

@@ -120,3 +120,29 @@ def test_strip_selection(gpu):
             s.set_stage_kernel("strip")
         assert s.stage_kernel() == "tile"
         s.run_steps(3)
+
+
+@pytest.mark.parametrize("case", ["mostly_dry", "dry_start"])
+def test_strip_dry_blocks_and_dynamic_schedule(gpu, case):
+    """Dry interior blocks write their zero slopes and faces instead of
+    computing them; once a step has skipped many of them, the next steps
+    claim blocks dynamically. The mostly-dry channel valley of the reference's
+    criterion bench (6% wet) and the valley flood from its dry start (rain
+    and inflow wet the blocks step by step) give the tile kernel's results
+    bit for bit."""
+    sim = gpu
+    from hydroflux_b200 import workloads
+    if case == "mostly_dry":
+        s = workloads.step_regime("mostly_dry", 512)
+        steps = 15
+    else:
+        s = workloads.valley(n=384, dx=5.0, seed=2, t_end=1e9)
+        steps = 25
+    out = {}
+    for kind in ("tile", "strip"):
+        with workloads.simulation_for(s) as sm:
+            sm.set_stage_kernel(kind)
+            sm.run_steps(steps, s.t_end)
+            out[kind] = (sm.states(), sm.steps(), sm.time())
+    assert out["tile"][1] == out["strip"][1] == steps and out["tile"][2] == out["strip"][2]
+    assert exact_fraction(out["strip"][0], out["tile"][0]) == 1.0
