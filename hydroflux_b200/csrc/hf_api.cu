@@ -374,26 +374,25 @@ int launch_sim_stage(hf_sim* s, bool second) {
   return launch_stage(a, s->grid, s->stream);
 }
 
-// Picks the stage kernel: the strip kernel where it is asked for (or, for
-// `kind` auto, where the grid has enough strip blocks per CTA) and its TMA
-// descriptors can be made, else the tile kernel.
+// Picks the stage kernel: the strip kernel where it is asked for and its TMA
+// descriptors can be made, else the tile kernel (also for `kind` auto: on
+// B200 the tile kernel measured faster on wet grids and as fast on mostly
+// dry ones).
 int choose_stage_kernel(hf_sim* s, int kind) {
   s->stage_kind = HF_STAGE_TILE;
-  if (kind == HF_STAGE_TILE) return HF_OK;
+  if (kind != HF_STAGE_STRIP) return HF_OK;
   int g = strip_grid_size(s->nr, s->nc, s->device);
-  if (g == 0 && kind == HF_STAGE_STRIP) {  // forced on a small grid: one CTA per block at most
+  if (g == 0) {  // a small grid: one CTA per block at most
     g = strip_grid_size(1 << 20, 1 << 12, s->device);
     const long long nq = (long long)strip_count(s->nc) * strip_blocks(s->nr);
     if (nq < g) g = (int)nq;
   }
-  if (g > 0 && strip_maps(stage_args(s, false), s->maps[0]) &&
-      strip_maps(stage_args(s, true), s->maps[1])) {
-    s->stage_kind = HF_STAGE_STRIP;
-    s->strip_grid = g;
-  } else if (kind == HF_STAGE_STRIP) {
+  if (!(g > 0 && strip_maps(stage_args(s, false), s->maps[0]) &&
+        strip_maps(stage_args(s, true), s->maps[1])))
     return fail(HF_ERR_UNSUPPORTED,
                 "the strip stage kernel needs an even column count and 16-byte aligned fields");
-  }
+  s->stage_kind = HF_STAGE_STRIP;
+  s->strip_grid = g;
   return HF_OK;
 }
 

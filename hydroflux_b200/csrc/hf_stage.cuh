@@ -7,6 +7,8 @@
 
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "hf_device.cuh"
 #include "hf_internal.h"
 
@@ -206,10 +208,11 @@ __device__ __forceinline__ void stage_prefetch(const StageArgs& A, StageSmem& S,
 }
 
 // ---------------------------------------------------------------------------
-// Per-item work of one forward-Euler stage, shared by the tile kernels (one
-// 32 x 8 tile and its halo at a time) and the strip kernel (a column of
-// blocks that carries the halo rows from one block to the next). Both keep
-// their arrays in shared memory with the same row widths and the same
+// Per-item work of one forward-Euler stage for the strip kernel (a column of
+// blocks that carries the halo rows from one block to the next). The same
+// arithmetic, in the same order, as the tile phases further below, which
+// keep it inline (written as one function per item, the tile kernel
+// measured 6% slower). The strip buffers use the tile's row widths and
 // offsets of row and column 0 (i4, i3, isx, ...); SM is the layout's type.
 // (gi0, gj0) is the grid cell of local (0, 0).
 // ---------------------------------------------------------------------------
@@ -509,15 +512,23 @@ __device__ __forceinline__ void update_at(const StageArgs& A, SM& S, int gi0, in
 // overlapping the alpha and update phases of this tile. `next` is a tile of
 // the grid described by *next_args (another scenario's, in an ensemble), or
 // of A when next_args is null.
-template <class T, bool PF = false, bool IN = false>
-__device__ __forceinline__ void stage_tile_faces(const StageArgs& A, StageSmemT<T>& S, int gi0,
+// DRY (forward stages of interior tiles only): when every depth of the tile
+// and its halo is at or below H_DRY, every cell of the tile takes the
+// isolated-dry update (update.rs:1072-1088), which reads no slope, face or
+// alpha: those phases are skipped and the function returns true. The vote
+// rides on the barrier that ends the primitives phase.
+template <class T, bool PF = false, bool IN = false, bool DRY = false>
+__device__ __forceinline__ bool stage_tile_faces(const StageArgs& A, StageSmemT<T>& S, int gi0,
                                                  int gj0, double dt, double* hst = nullptr,
                                                  int next = -1,
                                                  const StageArgs* next_args = nullptr) {
+  constexpr bool SKIP = DRY && IN;
+  bool dry = true;
   const int nr = A.nr, nc = A.nc;
   const double dx = A.dx, dy = A.dy;
   const double dt_dx = dt / dx;  // update.rs:930-931
   const double dt_dy = dt / dy;
+  const double half_dx = 0.5 * dx, half_dy = 0.5 * dy;
   const int tid = threadIdx.x;
   const T Z = cst<T>(0.0);
   if constexpr (PF) {
@@ -527,6 +538,7 @@ __device__ __forceinline__ void stage_tile_faces(const StageArgs& A, StageSmemT<
       const int r = k / R4W, cc = k - r * R4W;
       const double hh = hst[k];
       S.h[k] = hh;
+      if constexpr (SKIP) dry &= hh <= H_DRY;
       if (r >= 1 && r < R4H - 1 && cc >= 1 && cc < R4W - 1) {
         const int k3 = (r - 1) * R3W + (cc - 1);
         const double zz = S.eta[k3], qu = S.u[k3], qv = S.v[k3];
@@ -541,7 +553,14 @@ __device__ __forceinline__ void stage_tile_faces(const StageArgs& A, StageSmemT<
         S.v[k3] = vv;
       }
     }
-    __syncthreads();
+    if constexpr (SKIP) {
+      if (__syncthreads_and(dry)) {
+        if (next >= 0) stage_prefetch(next_args ? *next_args : A, S, hst, next);
+        return true;
+      }
+    } else {
+      __syncthreads();
+    }
   } else {
     // ---- depth snapshot (halo 4) and primitives (halo 3): update.rs:853-858, 405-426
     for (int k = tid; k < R4N; k += NTHREADS) {
@@ -568,30 +587,160 @@ __device__ __forceinline__ void stage_tile_faces(const StageArgs& A, StageSmemT<
         S.u[k3] = uu;
         S.v[k3] = vv;
       }
+      if constexpr (SKIP) dry &= val(hh) <= H_DRY;
     }
-    __syncthreads();
+    if constexpr (SKIP) {
+      if (__syncthreads_and(dry)) return true;
+    } else {
+      __syncthreads();
+    }
   }
   {
-    // slope item k < SXN: x slope at (k / SXW - 1, k % SXW - 2); else y slope
-    // at ((k - SXN) / SYW - 2, (k - SXN) % SYW - 1)
+    // ---- limited slopes: update.rs:459-540 (item k < SXN: x slope, else y)
     auto slope_item = [&](int k) {
-      if (k < SXN) {
+      const bool xd = k < SXN;
+      int li, lj;
+      if (xd) {
         const int r = k / SXW;
-        slope_at<T, IN>(A, S, gi0, gj0, r - 1, k - r * SXW - 2, true);
+        li = r - 1;
+        lj = k - r * SXW - 2;
       } else {
         const int kk = k - SXN, r = kk / SYW;
-        slope_at<T, IN>(A, S, gi0, gj0, r - 2, kk - r * SYW - 1, false);
+        li = r - 2;
+        lj = kk - r * SYW - 1;
+      }
+      const int gi = gi0 + li, gj = gj0 + lj;
+      if (!IN && (gi < 0 || gi >= nr || gj < 0 || gj >= nc)) return;
+      const int ga = xd ? gj : gi;
+      const int na = xd ? nc : nr;
+      const int st4 = xd ? 1 : R4W;
+      const int st3 = xd ? 1 : R3W;
+      const hfa::RecipD& rd = xd ? A.rx : A.ry;
+      T se = Z, su = Z, sv = Z;
+      if (IN || na >= 2) {
+        const int lo = IN ? -2 : max(ga - 2, 0) - ga, hi = IN ? 2 : min(ga + 2, na - 1) - ga;
+        const int c4 = i4(li, lj);
+        bool anyd = false;
+        for (int o = lo; o <= hi; ++o) anyd |= val(S.h[c4 + o * st4]) <= H_DRY;
+        if (!anyd) {
+          const int c3 = i3(li, lj);
+          if (!IN && ga == 0) {
+            const int r3 = c3 + st3;
+            se = dvr(S.eta[r3] - S.eta[c3], rd);  // / dx or / dy
+            su = dvr(S.u[r3] - S.u[c3], rd);
+            sv = dvr(S.v[r3] - S.v[c3], rd);
+          } else if (!IN && ga == na - 1) {
+            const int l3 = c3 - st3;
+            se = dvr(S.eta[c3] - S.eta[l3], rd);
+            su = dvr(S.u[c3] - S.u[l3], rd);
+            sv = dvr(S.v[c3] - S.v[l3], rd);
+          } else {
+            const int l3 = c3 - st3, r3 = c3 + st3;
+            se = minmod_div<T>(S.eta[c3] - S.eta[l3], S.eta[r3] - S.eta[c3], rd);
+            su = minmod_div<T>(S.u[c3] - S.u[l3], S.u[r3] - S.u[c3], rd);
+            sv = minmod_div<T>(S.v[c3] - S.v[l3], S.v[r3] - S.v[c3], rd);
+          }
+        }
+      }
+      if (xd) {
+        S.sxe[k] = se;
+        S.sxu[k] = su;
+        S.sxv[k] = sv;
+      } else {
+        S.sye[k - SXN] = se;
+        S.syu[k - SXN] = su;
+        S.syv[k - SXN] = sv;
       }
     };
-    // face item k < FXN: x face (row k / FXW - 1, face k % FXW - 1); else y
-    // face (face (k - FXN) / FYW - 1, column (k - FXN) % FYW - 1)
+
+    // ---- faces: update.rs:676-728 (face beds), 890-926 (fluxes) (item k < FXN: x face)
     auto face_item = [&](int k) {
-      if (k < FXN) {
+      const bool xd = k < FXN;
+      int li, lj;  // x face: (row li, face lj); y face: (face li, column lj)
+      if (xd) {
         const int r = k / FXW;
-        face_at<T, IN>(A, S, gi0, gj0, r - 1, k - r * FXW - 1, true);
+        li = r - 1;
+        lj = k - r * FXW - 1;
       } else {
         const int kk = k - FXN, r = kk / FYW;
-        face_at<T, IN>(A, S, gi0, gj0, r - 1, kk - r * FYW - 1, false);
+        li = r - 1;
+        lj = kk - r * FYW - 1;
+      }
+      const int gf = xd ? gj0 + lj : gi0 + li;  // face index along the normal
+      const int na = xd ? nc : nr;
+      const int gx = xd ? gi0 + li : gj0 + lj;  // index across
+      const int nx = xd ? nr : nc;
+      if (!IN && (gx < 0 || gx >= nx || gf < 0 || gf > na)) return;
+      const int mi = xd ? li : li - 1, mj = xd ? lj - 1 : lj;  // minus (left/top) cell
+      const int pi = li, pj = lj;                               // plus (right/bottom) cell
+      T m, nmn, npl, tg;
+      if (!IN && (gf == 0 || gf == na)) {
+        const bool lo_side = gf == 0;
+        const int ci = lo_side ? pi : mi, cj = lo_side ? pj : mj;
+        const int64_t g0 = (int64_t)(gi0 + ci) * nc + (gj0 + cj);
+        const T h = S.h[i4(ci, cj)];
+        const T hu = Field<T>::ld(A.in_hu, A.tan.in_hu, g0);
+        const T hv = Field<T>::ld(A.in_hv, A.tan.in_hv, g0);
+        int side;
+        int64_t g1;
+        double dn;
+        if (xd) {
+          side = lo_side ? SIDE_WEST : SIDE_EAST;
+          g1 = lo_side ? g0 + 1 : g0 - 1;
+          dn = dx;
+        } else {
+          side = lo_side ? SIDE_NORTH : SIDE_SOUTH;
+          g1 = lo_side ? g0 + nc : g0 - nc;
+          dn = dy;
+        }
+        const GhostT<T> G = ghost_cell<T>(side, A.bc, h, hu, hv, A.z, A.n, A.tan.n, g0, g1, dn);
+        const double zc = S.z[i3(ci, cj)];
+        const double zf = lo_side ? (G.z + zc) * 0.5 : (zc + G.z) * 0.5;
+        const T qn = xd ? hu : hv, qt = xd ? hv : hu;
+        const T gqn = xd ? G.hu : G.hv, gqt = xd ? G.hv : G.hu;
+        if (lo_side)
+          wb_face<T>(G.h, gqn, gqt, h, qn, qt, zf, m, nmn, npl, tg);
+        else
+          wb_face<T>(h, qn, qt, G.h, gqn, gqt, zf, m, nmn, npl, tg);
+      } else {
+        const T hm = S.h[i4(mi, mj)], hp = S.h[i4(pi, pj)];
+        const bool dm = val(hm) <= H_DRY, dp = val(hp) <= H_DRY;
+        if (dm && dp) {
+          m = Z; nmn = Z; npl = Z; tg = Z;
+        } else {
+          const int m3 = i3(mi, mj), p3 = i3(pi, pj);
+          const double zm = S.z[m3], zp = S.z[p3];
+          const double zf = (dm != dp) ? fmax(zm, zp) : (zm + zp) * 0.5;  // update.rs:650-656
+          const double half = xd ? half_dx : half_dy;
+          T se_m, sn_m, st_m, se_p, sn_p, st_p;
+          if (xd) {
+            const int a = isx(mi, mj), b = isx(pi, pj);
+            se_m = S.sxe[a]; sn_m = S.sxu[a]; st_m = S.sxv[a];
+            se_p = S.sxe[b]; sn_p = S.sxu[b]; st_p = S.sxv[b];
+          } else {
+            const int a = isy(mi, mj), b = isy(pi, pj);
+            se_m = S.sye[a]; sn_m = S.syv[a]; st_m = S.syu[a];
+            se_p = S.sye[b]; sn_p = S.syv[b]; st_p = S.syu[b];
+          }
+          const T un_mc = xd ? S.u[m3] : S.v[m3], ut_mc = xd ? S.v[m3] : S.u[m3];
+          const T un_pc = xd ? S.u[p3] : S.v[p3], ut_pc = xd ? S.v[p3] : S.u[p3];
+          // reconstruct_x/y_face_states (update.rs:560-623)
+          const T eta_m = S.eta[m3] + se_m * half;
+          const T un_m = un_mc + sn_m * half;
+          const T ut_m = ut_mc + st_m * half;
+          const T eta_p = S.eta[p3] - se_p * half;
+          const T un_p = un_pc - sn_p * half;
+          const T ut_p = ut_pc - st_p * half;
+          const T h_m = r_max(eta_m - zf, Z);
+          const T h_p = r_max(eta_p - zf, Z);
+          wb_face<T>(h_m, h_m * un_m, h_m * ut_m, h_p, h_p * un_p, h_p * ut_p, zf, m, nmn, npl, tg);
+        }
+      }
+      if (xd) {
+        S.fxm[k] = m; S.fxnm[k] = nmn; S.fxnp[k] = npl; S.fxt[k] = tg;
+      } else {
+        const int kk = k - FXN;
+        S.fym[kk] = m; S.fynm[kk] = nmn; S.fynp[kk] = npl; S.fyt[kk] = tg;
       }
     };
 
@@ -618,10 +767,21 @@ __device__ __forceinline__ void stage_tile_faces(const StageArgs& A, StageSmemT<
       const int r = k / AW;
       const int li = r - 1, lj = k - r * AW - 1;
       if ((li < 0 || li >= TY) && (lj < 0 || lj >= TX)) continue;
-      alpha_at<T, IN>(A, S, gi0, gj0, li, lj, dt_dx, dt_dy);
+      const int gi = gi0 + li, gj = gj0 + lj;
+      if (!IN && (gi < 0 || gi >= nr || gj < 0 || gj >= nc)) continue;
+      const T fr = S.fxm[ifx(li, lj + 1)], fl = S.fxm[ifx(li, lj)];
+      const T fb = S.fym[ify(li + 1, lj)], ft = S.fym[ify(li, lj)];
+      T out = Z;
+      if (val(fr) > 0.0) out = out + fr * dt_dx;
+      if (val(fl) < 0.0) out = out + (-fl) * dt_dx;
+      if (val(fb) > 0.0) out = out + fb * dt_dy;
+      if (val(ft) < 0.0) out = out + (-ft) * dt_dy;
+      const T avail = r_max(S.h[i4(li, lj)] - H_DRY, Z);
+      S.a[k] = (val(out) > val(avail) && val(out) > 0.0) ? dvp(avail, out) : cst<T>(1.0);
     }
     __syncthreads();
   }
+  return false;
 }
 
 // One forward-Euler stage (update.rs:805-1211) on one tile of one grid. Called
@@ -634,23 +794,122 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, StageSmemT<T>& S,
                                            double& sxm, double& sym, unsigned long long& nonfin,
                                            double* hst = nullptr, int next = -1,
                                            const StageArgs* next_args = nullptr) {
-  const double dt = A.ctrl->dt;
-  const double dt_dx = dt / A.dx;  // update.rs:930-931
-  const double dt_dy = dt / A.dy;
+  Ctrl* ctrl = A.ctrl;
+  const double dt = ctrl->dt;
+  const int nr = A.nr, nc = A.nc;
+  const double dx = A.dx, dy = A.dy;
+  const double dt_dx = dt / dx;  // update.rs:930-931
+  const double dt_dy = dt / dy;
   const int tid = threadIdx.x;
-  const int tyi = tile / A.tiles_x;
-  const int gi0 = tyi * TY, gj0 = (tile - tyi * A.tiles_x) * TX;
-  stage_tile_faces<T, PF, IN>(A, S, gi0, gj0, dt, hst, next, next_args);
-  int src_lo = 0, src_hi = 0;
-  if (A.finalize && A.f.n_src > 0) {
-    src_lo = A.f.tile_start[tile];
-    src_hi = A.f.tile_start[tile + 1];
-  }
+  const T Z = cst<T>(0.0);
+  {
+    const int tyi = tile / A.tiles_x;
+    const int gi0 = tyi * TY, gj0 = (tile - tyi * A.tiles_x) * TX;
+    // Dry interior tiles skip their slopes, faces and alpha (f64 forward stage).
+  stage_tile_faces<T, PF, IN, std::is_same<T, double>::value>(A, S, gi0, gj0, dt, hst, next,
+                                                                 next_args);
+
+    // ---- FV update + bed source + floor: update.rs:1071-1210
+    int src_lo = 0, src_hi = 0;
+    if (A.finalize && A.f.n_src > 0) {
+      src_lo = A.f.tile_start[tile];
+      src_hi = A.f.tile_start[tile + 1];
+    }
 #pragma unroll 1
-  for (int q = 0; q < CELLS_PER_THREAD; ++q)
-    update_at<T, IN>(A, S, gi0, gj0, tid / TX + ROWS_PER_PASS * q, tid % TX, dt, dt_dx, dt_dy,
-                     A.f.tile_order, src_lo, src_hi, sxm, sym, nonfin);
-  __syncthreads();
+    for (int q = 0; q < CELLS_PER_THREAD; ++q) {
+      const int li = tid / TX + ROWS_PER_PASS * q, lj = tid % TX;
+      const int gi = gi0 + li, gj = gj0 + lj;
+      if (!IN && (gi >= nr || gj >= nc)) continue;
+      const int64_t g = (int64_t)gi * nc + gj;
+      const int c4 = i4(li, lj), c3 = i3(li, lj);
+      const T hc = S.h[c4];
+      const bool dc = val(hc) <= H_DRY;
+      T nh, nhu, nhv;
+      if (dc && (IN || (gi > 0 && gi + 1 < nr && gj > 0 && gj + 1 < nc)) && val(S.h[c4 - R4W]) <= H_DRY &&
+          val(S.h[c4 + R4W]) <= H_DRY && val(S.h[c4 - 1]) <= H_DRY && val(S.h[c4 + 1]) <= H_DRY) {
+        nh = hc;  // isolated-dry fast path (update.rs:1072-1088)
+        nhu = Z;
+        nhv = Z;
+      } else {
+        const int fr = ifx(li, lj + 1), fl = ifx(li, lj), fb = ify(li + 1, lj), ft = ify(li, lj);
+        const T mr = S.fxm[fr], ml = S.fxm[fl], mb = S.fym[fb], mt = S.fym[ft];
+        const T ac = S.a[ia(li, lj)];
+        const T one = cst<T>(1.0);
+        // Upstream alpha per face (update.rs:992-1053). Dry-dry interior faces
+        // are exact zeros; scaling them by an alpha in [0, 1] keeps them +0.
+        const T ar = (!IN && gj + 1 == nc) ? (val(mr) > 0.0 ? ac : one) : (val(mr) > 0.0 ? ac : S.a[ia(li, lj + 1)]);
+        const T al = (!IN && gj == 0) ? (val(ml) < 0.0 ? ac : one) : (val(ml) > 0.0 ? S.a[ia(li, lj - 1)] : ac);
+        const T ab = (!IN && gi + 1 == nr) ? (val(mb) > 0.0 ? ac : one) : (val(mb) > 0.0 ? ac : S.a[ia(li + 1, lj)]);
+        const T at = (!IN && gi == 0) ? (val(mt) < 0.0 ? ac : one) : (val(mt) > 0.0 ? S.a[ia(li - 1, lj)] : ac);
+        const T fxr_m = mr * ar, fxr_n = S.fxnm[fr] * ar, fxr_t = S.fxt[fr] * ar;
+        const T fxl_m = ml * al, fxl_n = S.fxnp[fl] * al, fxl_t = S.fxt[fl] * al;
+        const T fyb_m = mb * ab, fyb_n = S.fynm[fb] * ab, fyb_t = S.fyt[fb] * ab;
+        const T fyt_m = mt * at, fyt_n = S.fynp[ft] * at, fyt_t = S.fyt[ft] * at;
+        const T dh = (fxr_m - fxl_m) * dt_dx + (fyb_m - fyt_m) * dt_dy;
+        const T new_h = hc - dh;
+        const T dhu = (fxr_n - fxl_n) * dt_dx + (fyb_t - fyt_t) * dt_dy;
+        const T dhv = (fxr_t - fxl_t) * dt_dx + (fyb_n - fyt_n) * dt_dy;
+
+        double zfl, zfr, zft, zfb;
+        cell_face_beds<IN>(A, S.z, dc, val(S.h[c4 - 1]) <= H_DRY, val(S.h[c4 + 1]) <= H_DRY,
+                       val(S.h[c4 - R4W]) <= H_DRY, val(S.h[c4 + R4W]) <= H_DRY, c3, gi, gj, zfl,
+                       zfr, zft, zfb);
+
+        // Explicit bed-slope source on the reconstructed face states (update.rs:1140-1180).
+        const double zc = S.z[c3];
+        const T eta_cell = hc + zc;
+        const T sex = S.sxe[isx(li, lj)];
+        const T eta_left = (IN || gj > 0) ? eta_cell - sex * (0.5 * dx) : eta_cell;
+        const T eta_right = (IN || gj + 1 < nc) ? eta_cell + sex * (0.5 * dx) : eta_cell;
+        const T hfl = r_max(eta_left - zfl, Z);
+        const T hfr = r_max(eta_right - zfr, Z);
+        const T s_hu = dvr((hfl + hfr) * ((eta_left - hfl) - (eta_right - hfr)) * (0.5 * GRAVITY), A.rx);
+        const T sey = S.sye[isy(li, lj)];
+        const T eta_top = (IN || gi > 0) ? eta_cell - sey * (0.5 * dy) : eta_cell;
+        const T eta_bot = (IN || gi + 1 < nr) ? eta_cell + sey * (0.5 * dy) : eta_cell;
+        const T hft = r_max(eta_top - zft, Z);
+        const T hfb = r_max(eta_bot - zfb, Z);
+        const T s_hv = dvr((hft + hfb) * ((eta_top - hft) - (eta_bot - hfb)) * (0.5 * GRAVITY), A.ry);
+
+        if (val(new_h) <= H_VEL) {
+          nh = r_max(new_h, Z);  // moisture floor keeps the mass
+          nhu = Z;
+          nhv = Z;
+        } else {
+          T hu_old = Z, hv_old = Z;
+          if (val(hc) > H_VEL) {
+            hu_old = Field<T>::ld(A.in_hu, A.tan.in_hu, g);
+            hv_old = Field<T>::ld(A.in_hv, A.tan.in_hv, g);
+          }
+          nh = new_h;
+          nhu = hu_old - dhu + s_hu * dt;
+          nhv = hv_old - dhv + s_hv * dt;
+        }
+      }
+      if (A.combine) {  // SSP-RK2 convex combination + floor (update.rs:1271-1286)
+        const T ph = Field<T>::ld(A.un_h, A.tan.un_h, g);
+        const T phu = Field<T>::ld(A.un_hu, A.tan.un_hu, g);
+        const T phv = Field<T>::ld(A.un_hv, A.tan.un_hv, g);
+        nh = (ph + nh) * 0.5;
+        nhu = (phu + nhu) * 0.5;
+        nhv = (phv + nhv) * 0.5;
+        if (val(nh) <= H_VEL) {
+          nh = r_max(nh, Z);
+          nhu = Z;
+          nhv = Z;
+        }
+      }
+      if (A.finalize) {
+        finalize_cell<T>(A, ctrl, dt, gi, gj, g, A.f.tile_order, src_lo, src_hi, nh, nhu, nhv);
+        cfl_cell<IN>(A, gi, gj, g, val(nh), val(nhu), val(nhv), sxm, sym);
+        if (ctrl->check_finite && !isfinite(val(nh))) ++nonfin;
+      }
+      Field<T>::st(A.out_h, A.tan.out_h, g, nh);
+      Field<T>::st(A.out_hu, A.tan.out_hu, g, nhu);
+      Field<T>::st(A.out_hv, A.tan.out_hv, g, nhv);
+    }
+    __syncthreads();
+  }
 }
 
 // A tile whose 4-cell halo lies inside the grid reaches no side: it runs the

@@ -164,10 +164,10 @@ int hf_sim_set_boundaries(hf_sim* sim, const hf_boundaries* bcs);
  * tile with its halo; HF_STAGE_STRIP walks 32-column strips in 7-row blocks
  * and carries the halo rows from block to block (fewer faces and slopes per
  * cell, TMA row fetches; needs an even column count). HF_STAGE_AUTO (the
- * default at creation) takes the strip kernel when the grid has enough
- * strip blocks per CTA. Results are bit-identical; this is a tuning and
- * diagnostic knob. Forcing HF_STAGE_STRIP where it cannot run returns
- * HF_ERR_UNSUPPORTED (the tile kernel stays selected). */
+ * default at creation) takes the tile kernel, which measured faster on B200.
+ * Results are bit-identical; this is a tuning and diagnostic knob. Forcing
+ * HF_STAGE_STRIP where it cannot run returns HF_ERR_UNSUPPORTED (the tile
+ * kernel stays selected). */
 enum { HF_STAGE_AUTO = 0, HF_STAGE_TILE = 1, HF_STAGE_STRIP = 2 };
 int hf_sim_set_stage_kernel(hf_sim* sim, int kind);
 int hf_sim_stage_kernel(const hf_sim* sim, int* kind);

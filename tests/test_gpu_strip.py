@@ -98,12 +98,14 @@ def test_strip_forcing_against_oracle(gpu, oracle, integrator):
 
 
 def test_strip_selection(gpu):
-    """The default picks the strip kernel on a large grid and the tile
-    kernel on a small one; an odd column count cannot use it."""
+    """The default is the tile kernel; the strip kernel is taken when asked
+    for, on any grid with an even column count."""
     sim = gpu
     zero = np.zeros((2048, 2048))
     with sim.Simulation(sim.Mesh2D(zero, 1.0, 1.0, 0.03), (zero + 1.0, zero, zero),
                         sim.SimulationConfig()) as s:
+        assert s.stage_kernel() == "tile"
+        s.set_stage_kernel("strip")
         assert s.stage_kernel() == "strip"
     small = np.zeros((64, 64))
     with sim.Simulation(sim.Mesh2D(small, 1.0, 1.0, 0.03), (small + 1.0, small, small),
