@@ -49,6 +49,8 @@ def parse():
     p.add_argument("--cpu-steps", type=int, default=2, help="oracle steps in the CPU baseline")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--stage-kernel", default="auto", choices=["auto", "tile", "strip"],
+                   help="valley: the stage kernel (hf_sim_set_stage_kernel; bit-identical)")
     p.add_argument("--workload", default="valley", choices=["valley", "ensemble", "adjoint",
                                                             "serve", "lanes", "regimes"],
                    help="valley: the 4096^2 plain step (default line); ensemble: batched "
@@ -224,6 +226,7 @@ def run_ours(a, d: Dist):
     cells = scn.n_cells
 
     sm = workloads.simulation_for(scn, device=dev)
+    sm.set_stage_kernel(a.stage_kernel)
     h_d, hu_d, hv_d, stream_ptr = sm.device_state()
     stream = torch.cuda.ExternalStream(stream_ptr, device=dev)
     sm.run_steps(max(a.warmup, 3), scn.t_end)
@@ -284,6 +287,7 @@ def run_ours(a, d: Dist):
         mesh = S.Mesh2D(bed_p.numpy(), scn_w.dx, scn_w.dy, man_p.numpy())
         st = tuple(p_.numpy() for p_ in pinned)
         s2 = S.Simulation(mesh, st, cfg, dev)
+        s2.set_stage_kernel(a.stage_kernel)
         s2.set_rain(np.stack(scn_w.rain, axis=1))
         s2.set_point_sources([S.PointSource(r, c, np.stack([t, q], axis=1))
                               for r, c, t, q in scn_w.sources])

@@ -219,6 +219,69 @@ def test_gradient_against_central_differences(gpu):
             assert abs(fd - ad) <= 2e-5 * abs(ad), (k, fd, ad)
 
 
+def test_gradient_fd_converges_on_a_smooth_run(gpu):
+    """Central differences converge to the adjoint to 1e-6 where the run is
+    smooth: a 32 x 32 bump of water 1 to 1.4 m deep, all wet, 40 steps, no
+    cell near the dry or velocity thresholds, dt frozen. At eps = 1e-5 (a
+    relative perturbation of n) FD's truncation and J's rounding (about
+    1e-15 |J| / eps) are both far below 1e-6."""
+    calib, workloads = gpu
+    nr = nc = 32
+    K = 40
+    xx, yy = np.meshgrid(np.arange(nc) + 0.5, np.arange(nr) + 0.5)
+    h = 1.0 + 0.4 * np.exp(-((xx - nc * 0.45) ** 2 + (yy - nr * 0.53) ** 2) / (nr * 1.0))
+    z = 0.01 * xx
+    rng = np.random.default_rng(6)
+    n = lognormal(rng, (nr, nc), median=0.05)
+    s = workloads.Scenario("bump", z, n, 1.0, 1.0, h, np.zeros_like(h), np.zeros_like(h),
+                           bcs=((0, 0.0),) * 4, cfl=0.4, t_end=1e9, max_dt=1.0)
+    gauges = np.array([5 * nc + 5, (nr // 2) * nc + nc // 2, (nr - 7) * nc + 9])
+    with calib.Calibration(s, K, gauges) as cal:
+        obs = np.zeros((K, len(gauges)))
+        obs[:] = 1.1
+        cal.set_observations(obs)
+        _, g = cal.gradient(n)
+        for k in range(3):
+            v = rng.standard_normal(n.shape)
+            ad = float(np.sum(g * n * v))
+            cal.run(n)  # the dt record of the base field
+            eps = 1e-5
+            Jp, _, _ = cal.run(n + eps * n * v, replay_dt=True)
+            Jm, _, _ = cal.run(n - eps * n * v, replay_dt=True)
+            fd = (Jp - Jm) / (2 * eps)
+            assert abs(fd - ad) <= 1e-6 * abs(ad), (k, fd, ad)
+
+
+def test_gradient_fd_on_the_calibration_problem(gpu):
+    """The 512 x 512 valley misfit at 100 steps (the flood wetting the
+    valley): FD agrees with the adjoint to 1e-4 at every eps from 1e-6 to
+    1e-7, but no closer at any eps. The discrete step is discontinuous where
+    a cell crosses the velocity floor (update.rs: momentum set to zero at
+    h <= H_VEL) or the dry-cell paths, so J(n) has small jumps and central
+    differences carry an error of ~1e-5 that does not shrink with eps; the
+    adjoint is the derivative of the smooth pieces, the Dual's (it matches
+    the tangent to 1e-13)."""
+    calib, workloads = gpu
+    K = 100
+    P = workloads.calibration_problem(n=512, n_steps=K)
+    s = P.scenario
+    with calib.Calibration(s, K, P.gauges) as cal:
+        _, gh, ko = cal.run(P.manning_true)
+        ob = np.zeros((K, len(P.gauges)))
+        ob[:ko] = gh
+        cal.set_observations(ob)
+        _, g = cal.gradient(s.manning)
+        for d in range(3):
+            v = np.random.default_rng(100 + d).standard_normal(s.shape) * s.manning
+            ad = float(np.sum(g * v))
+            cal.run(s.manning)
+            for eps in (1e-6, 3e-7, 1e-7):
+                Jp, _, _ = cal.run(s.manning + eps * v, replay_dt=True)
+                Jm, _, _ = cal.run(s.manning - eps * v, replay_dt=True)
+                fd = (Jp - Jm) / (2 * eps)
+                assert abs(fd - ad) <= 1e-4 * abs(ad), (d, eps, fd, ad)
+
+
 @pytest.mark.parametrize("name", PROBLEMS)
 def test_tangent_lanes_equal_single_tangents(gpu, name):
     """Vector mode (DualN, autograd/src/dual_n.rs): every lane of one
