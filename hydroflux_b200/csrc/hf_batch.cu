@@ -93,6 +93,10 @@ struct hf_batch {
   int* d_tile_local = nullptr;      // tile index within its scenario, order 0
   int* d_tile_local_lpt = nullptr;  // order 1
   int* d_counters = nullptr;        // dynamic schedule: stage 1 / stage 2 tile counters
+  // Scenarios still running when the tile lists were last built: finished
+  // scenarios' tiles are dropped from the lists (they would only be skipped).
+  int64_t listed = -1;
+  std::vector<int> tiles_of;  // tiles per scenario
   cudaGraphExec_t graphs[kSchedules][3] = {};
   int schedule = -1;  // -1: not tuned yet
   int forced = -1;    // hf_batch_set_schedule
@@ -124,7 +128,7 @@ void destroy_batch(hf_batch* b) {
 int enqueue_batch_step(hf_batch* b, int sched) {
   const bool dynamic = sched & 1, lpt = sched & 2;
   const int* scn = lpt ? b->d_tile_scn_lpt : b->d_tile_scn;
-  const int* local = lpt ? b->d_tile_local_lpt : (dynamic ? b->d_tile_local : nullptr);
+  const int* local = lpt ? b->d_tile_local_lpt : b->d_tile_local;
   int* c1 = dynamic ? b->d_counters : nullptr;
   int* c2 = dynamic ? b->d_counters + 1 : nullptr;
   if (launch_batch_control(b->d_ctrl, b->d_args1, b->n, b->stream, dynamic ? b->d_counters : nullptr))
@@ -168,6 +172,39 @@ int64_t count_unfinished(const hf_batch* b) {
   return k;
 }
 
+// Rebuilds the two tile lists (scenario order; largest first) over the
+// scenarios that are still running, in place: the graphs read the lists and
+// their length from device memory, so they stay valid. Results do not
+// change: a finished scenario's tiles are skipped by the kernel anyway.
+int compact_tile_lists(hf_batch* b) {
+  std::vector<int> order0, order1, scn0, loc0, scn1, loc1;
+  for (int s = 0; s < b->n; ++s)
+    if (b->h_ctrl[s].status == 0 && b->h_ctrl[s].t < b->t_end[s]) order0.push_back(s);
+  order1 = order0;
+  std::stable_sort(order1.begin(), order1.end(),
+                   [&](int x, int y) { return b->tiles_of[x] > b->tiles_of[y]; });
+  for (int s : order0)
+    for (int t = 0; t < b->tiles_of[s]; ++t) {
+      scn0.push_back(s);
+      loc0.push_back(t);
+    }
+  for (int s : order1)
+    for (int t = 0; t < b->tiles_of[s]; ++t) {
+      scn1.push_back(s);
+      loc1.push_back(t);
+    }
+  const int nt = (int)scn0.size();
+  if (nt > 0 &&
+      (cudaMemcpy(b->d_tile_scn, scn0.data(), nt * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
+       cudaMemcpy(b->d_tile_local, loc0.data(), nt * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
+       cudaMemcpy(b->d_tile_scn_lpt, scn1.data(), nt * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
+       cudaMemcpy(b->d_tile_local_lpt, loc1.data(), nt * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess))
+    return bcuda(failed_call_error(), "compact tile lists");
+  if (cudaMemcpy(b->d_n_tiles, &nt, sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+    return bcuda(failed_call_error(), "compact tile lists");
+  return HF_OK;
+}
+
 // One graph chunk of schedule `sched`, then the control blocks read back.
 // elapsed_ms (optional): device time of the chunk.
 int run_chunk(hf_batch* b, int sched, int which, int64_t* running, float* elapsed_ms) {
@@ -191,6 +228,10 @@ int run_chunk(hf_batch* b, int sched, int which, int64_t* running, float* elapse
   *running = count_unfinished(b);
   if (*running > 0 && total_steps(b) == steps_before)  // would repeat forever
     return bfail(HF_ERR_TIMEOUT, "ensemble made no progress: no scenario took a step");
+  if (*running > 0 && *running < b->listed) {
+    B_TRY(compact_tile_lists(b));
+    b->listed = *running;
+  }
   return HF_OK;
 }
 
@@ -328,9 +369,11 @@ int hf_batch_create(int64_t n_scenarios, const hf_scenario_desc* sc, int device,
       tile_scn[tb + t] = s;
       tile_local[tb + t] = t;
     }
+    b->tiles_of.push_back(tx * ty);
     tb += tx * ty;
     o += ncell;
   }
+  b->listed = b->n;
   // Order 1: the same tiles, scenarios by decreasing tile count (stable).
   std::vector<int> by_size(b->n), tile_scn_lpt, tile_local_lpt;
   for (int s = 0; s < b->n; ++s) by_size[s] = s;

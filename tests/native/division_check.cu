@@ -3,9 +3,11 @@
 //   hfa::div_recip  (reciprocal + Markstein correction, fixed divisor)
 //   hfa::div_rn     (zero-safe a / b)
 //   hfa::div_rn_pos (a / b for b > 0)
-// Inputs: counter-based random pairs; divisors from typical grid spacings and
-// random ones; numerators over the whole exponent range with extra weight on
-// the edges of div_recip's fast-path window, zeros, subnormals, infinities.
+// Inputs: counter-based random pairs; divisors from typical grid spacings,
+// random ones within 2^+-100, and ones with exponents anywhere within 2^+-520
+// (weighted towards 2^+-500); numerators over the whole exponent range with
+// extra weight on the edges of div_recip's fast-path window and on
+// 2^+-500, zeros, subnormals, infinities.
 #include <cstdio>
 #include <cuda_runtime.h>
 
@@ -33,15 +35,20 @@ __global__ void k_check(unsigned long long seed, long long n, int dmode,
     if (dmode == 0) {
       const double sp[8] = {1.0, 2.0, 5.0, 10.0, 30.0, 0.1, 3.7, 0.25};
       d = sp[r2 & 7];
-    } else {
+    } else if (dmode == 1) {
       const unsigned long long e = 1023 - 100 + (r2 % 201);
+      d = __longlong_as_double((long long)((e << 52) | ((r2 >> 11) & 0xFFFFFFFFFFFFFull)));
+    } else {  // wide divisors, weighted towards 2^+-500
+      const unsigned long long e = (r2 & 1) ? 1023 - 520 + (r2 % 1041)
+                                            : ((r2 & 2) ? 523 - 8 : 1523 - 8) + (r2 >> 56) % 17;
       d = __longlong_as_double((long long)((e << 52) | ((r2 >> 11) & 0xFFFFFFFFFFFFFull)));
     }
     unsigned long long ea;
     const unsigned sel = (unsigned)(r1 >> 60);
-    if (sel < 8) ea = 1023 - 60 + ((r1 >> 40) % 120);
-    else if (sel < 11) ea = 1023 - 705 + ((r1 >> 40) % 12);
-    else if (sel < 13) ea = 1023 + 895 + ((r1 >> 40) % 12);
+    if (sel < 7) ea = 1023 - 60 + ((r1 >> 40) % 120);
+    else if (sel < 9) ea = 1023 - 705 + ((r1 >> 40) % 12);
+    else if (sel < 11) ea = 1023 + 895 + ((r1 >> 40) % 12);
+    else if (sel < 13) ea = ((r1 >> 38) & 1 ? 523 - 8 : 1523 - 8) + ((r1 >> 40) % 17);
     else ea = (r1 >> 40) % 2048;  // anything: zeros, subnormals, inf / NaN
     const double a = __longlong_as_double(
         (long long)(((r1 & 1ull) << 63) | (ea << 52) | ((r1 >> 1) & 0xFFFFFFFFFFFFFull)));
@@ -70,7 +77,7 @@ int main(int argc, char** argv) {
   unsigned long long* counts = nullptr;
   if (cudaMalloc(&counts, 4 * sizeof(unsigned long long)) != cudaSuccess) return 2;
   int fails = 0;
-  for (int dmode = 0; dmode < 2; ++dmode)
+  for (int dmode = 0; dmode < 3; ++dmode)
     for (unsigned long long seed = 1; seed <= 2; ++seed) {
       cudaMemset(counts, 0, 4 * sizeof(unsigned long long));
       k_check<<<148 * 8, 256>>>(seed + 10 * dmode, n, dmode, counts);
@@ -78,7 +85,8 @@ int main(int argc, char** argv) {
       if (cudaMemcpy(h, counts, sizeof h, cudaMemcpyDeviceToHost) != cudaSuccess) return 2;
       printf("divisors %s, seed %llu: %lld pairs (%llu on the reciprocal fast path); "
              "mismatches div_recip %llu, div_rn_pos %llu, div_rn %llu\n",
-             dmode ? "random" : "spacings", seed, n, h[3], h[0], h[1], h[2]);
+             dmode == 0 ? "spacings" : (dmode == 1 ? "random" : "window"), seed, n, h[3], h[0],
+             h[1], h[2]);
       fails += (h[0] || h[1] || h[2]);
     }
   return fails ? 1 : 0;
