@@ -212,9 +212,8 @@ __global__ void __launch_bounds__(NTHREADS, HF_MIN_BLOCKS)
 // One stage of every grid of an ensemble in one launch: the persistent grid
 // walks the concatenated tile list of all scenarios; tile t belongs to
 // scenario tile_scn[t], whose arguments (own sizes, dt, forcings, control
-// block) are args[tile_scn[t]]. Finished scenarios' tiles are skipped. The
-// CFL maxima are reduced per tile into the tile's scenario; each scenario's
-// clock is committed afterwards by k_batch_commit.
+// block) are args[tile_scn[t]]. Finished scenarios' tiles are skipped; each
+// scenario's clock is committed afterwards by k_batch_commit.
 //
 // Schedules (the ensemble's autotuner picks one): tile_local == nullptr
 // means tile t is tile t - tile_base of its scenario, else tile_local[t]
@@ -223,17 +222,15 @@ __global__ void __launch_bounds__(NTHREADS, HF_MIN_BLOCKS)
 // counter (dynamic; k_batch_control zeroes it before each step). Results do
 // not depend on the schedule: tiles are independent and the CFL reduction is
 // a max.
-__device__ __forceinline__ void batch_tile(const StageArgs* __restrict__ args,
-                                           const int* __restrict__ tile_scn,
-                                           const int* __restrict__ tile_local, int t,
-                                           StageSmem& S) {
-  const StageArgs& A = args[tile_scn[t]];
-  if (!A.ctrl->active) return;  // uniform over the CTA
-  double sxm = 0.0, sym = 0.0;
-  unsigned long long nonfin = 0;
-  stage_tile_any<double>(A, S, tile_local ? tile_local[t] : t - A.tile_base, sxm, sym, nonfin);
-  if (A.finalize) block_reduce_speeds(sxm, sym, nonfin, A.ctrl);
-}
+//
+// Either way the walk is software-pipelined like k_stage_pf: a CTA knows its
+// next tile before it computes the current one, and the next tile's inputs
+// (of whichever scenario it belongs to) are copied into shared memory while
+// the current tile's alpha and update phases run. The arguments of the
+// scenario in hand sit in shared memory (copied when the walk enters another
+// scenario: consecutive tiles of a CTA mostly share one), and its CFL maxima
+// are reduced into its control block once per run of its tiles, not per tile.
+static_assert(sizeof(StageArgs) % 8 == 0, "StageArgs is copied in 8-byte words");
 
 __global__ void __launch_bounds__(NTHREADS, HF_MIN_BLOCKS)
     k_stage_batch(const StageArgs* __restrict__ args, const int* __restrict__ tile_scn,
@@ -241,49 +238,62 @@ __global__ void __launch_bounds__(NTHREADS, HF_MIN_BLOCKS)
                   int* counter) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   StagePfSmem& P = *reinterpret_cast<StagePfSmem*>(smem_raw);
-  const int total_tiles = *n_tiles;  // device-resident: a graph serves any set of scenarios
-  if (counter == nullptr) {
-    for (int t = blockIdx.x; t < total_tiles; t += gridDim.x)
-      batch_tile(args, tile_scn, tile_local, t, P.s);
-    return;
-  }
-  // Dynamic schedule, software-pipelined like k_stage_pf: a CTA claims its
-  // next tile from the counter before it computes the current one, and the
-  // next tile's inputs (of whichever scenario it belongs to) are copied into
-  // shared memory while the current tile's alpha and update phases run.
+  __shared__ __align__(16) unsigned char args_raw[sizeof(StageArgs)];
+  StageArgs& A = *reinterpret_cast<StageArgs*>(args_raw);
   __shared__ int claimed;
-  if (threadIdx.x == 0) claimed = atomicAdd(counter, 1);
-  __syncthreads();
-  int t = claimed;
+  const int total_tiles = *n_tiles;  // device-resident: a graph serves any set of scenarios
+  int t = blockIdx.x;
+  if (counter) {
+    if (threadIdx.x == 0) claimed = atomicAdd(counter, 1);
+    __syncthreads();
+    t = claimed;
+  }
   if (t < total_tiles) {
     const StageArgs& A0 = args[tile_scn[t]];
     if (A0.ctrl->active) stage_prefetch(A0, P.s, P.hst, tile_local ? tile_local[t] : t - A0.tile_base);
   }
   __syncthreads();  // every thread has read `claimed`
+  int cur = -1;     // scenario whose arguments are in A
+  bool live = false;
+  double sxm = 0.0, sym = 0.0;
+  unsigned long long nonfin = 0;
   while (t < total_tiles) {
-    if (threadIdx.x == 0) claimed = atomicAdd(counter, 1);
+    const int scn = tile_scn[t];
+    if (scn != cur) {  // uniform over the CTA
+      if (live && A.finalize) block_reduce_speeds(sxm, sym, nonfin, A.ctrl);
+      sxm = sym = 0.0;
+      nonfin = 0;
+      __syncthreads();  // nobody reads the old arguments any more
+      const unsigned long long* src = reinterpret_cast<const unsigned long long*>(&args[scn]);
+      unsigned long long* dst = reinterpret_cast<unsigned long long*>(args_raw);
+      for (int w = threadIdx.x; w < (int)(sizeof(StageArgs) / 8); w += NTHREADS) dst[w] = src[w];
+      cur = scn;
+    }
+    if (counter && threadIdx.x == 0) claimed = atomicAdd(counter, 1);
     cp_async_wait_all();
-    __syncthreads();  // this tile's inputs are in shared memory; the claim is visible
-    const int tn = claimed;
-    const StageArgs& A = args[tile_scn[t]];
-    const StageArgs* An = tn < total_tiles ? &args[tile_scn[tn]] : nullptr;
-    if (An && !An->ctrl->active) An = nullptr;  // finished scenario: nothing to fetch
+    __syncthreads();  // this tile's inputs and A are in shared memory; the claim is visible
+    live = A.ctrl->active != 0;  // uniform over the CTA
+    const int tn = counter ? claimed : t + (int)gridDim.x;
+    const StageArgs* An = nullptr;
+    if (tn < total_tiles) {
+      const int sn = tile_scn[tn];
+      An = sn == cur ? &A : &args[sn];
+      if (!An->ctrl->active) An = nullptr;  // finished scenario: nothing to fetch
+    }
     const int ln = An ? (tile_local ? tile_local[tn] : tn - An->tile_base) : -1;
-    if (A.ctrl->active) {  // uniform over the CTA
+    if (live) {
       const int tile = tile_local ? tile_local[t] : t - A.tile_base;
-      double sxm = 0.0, sym = 0.0;
-      unsigned long long nonfin = 0;
       if (interior_tile(A, tile))
         stage_tile<double, true, true>(A, P.s, tile, sxm, sym, nonfin, P.hst, ln, An);
       else
         stage_tile<double, true>(A, P.s, tile, sxm, sym, nonfin, P.hst, ln, An);
-      if (A.finalize) block_reduce_speeds(sxm, sym, nonfin, A.ctrl);
     } else if (An) {
       stage_prefetch(*An, P.s, P.hst, ln);
     }
     __syncthreads();  // every thread has read `claimed` before thread 0 takes another
     t = tn;
   }
+  if (live && A.finalize) block_reduce_speeds(sxm, sym, nonfin, A.ctrl);
 }
 
 // Epilogue of a forward-Euler step: friction, forcings and the CFL
