@@ -215,6 +215,13 @@ def cpu_baseline(scn, state, t0, steps, threads):
 
 
 # -------------------------------------------------------------- ours (GPU)
+def launches() -> int:
+    """Kernels the library has launched so far in this process (its own
+    count: direct launches plus every kernel node of each graph launch)."""
+    from hydroflux_b200 import _lib
+    return _lib.kernel_launches()
+
+
 def run_ours(a, d: Dist):
     import torch
 
@@ -248,7 +255,9 @@ def run_ours(a, d: Dist):
     e1 = torch.cuda.Event(enable_timing=True)
     with torch.cuda.stream(stream):
         e0.record(stream)
+    k_launch = launches()
     sm.run_steps(a.steps, scn.t_end)
+    k_launch = launches() - k_launch
     with torch.cuda.stream(stream):
         e1.record(stream)
     torch.cuda.synchronize(dev)
@@ -329,7 +338,7 @@ def run_ours(a, d: Dist):
         "data": "synthetic (seeded valley DEM, Voronoi Manning field, rain + inflow hydrograph)",
         "config": valley_config(a, d.world, wet_frac),
         "e2e": e2e,
-        "gpu_launches": 3 * a.steps,
+        "gpu_launches": k_launch,
         "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
                      "frac": achieved_gbs / peak, "peak_source": peak_kind,
                      "traffic": (traffic_per_cell * cells) if traffic_per_cell else None,
@@ -404,6 +413,7 @@ def run_regimes(a, d: Dist):
     out = {}
     clocks = ClockSampler(dev)
     clocks.start()
+    k_launch = 0
     for kind in ("mostly_dry", "all_wet"):
         scn = workloads.step_regime(kind, a.n)
         with workloads.simulation_for(scn, device=dev) as sm:
@@ -417,7 +427,9 @@ def run_regimes(a, d: Dist):
             e1 = torch.cuda.Event(enable_timing=True)
             with torch.cuda.stream(stream):
                 e0.record(stream)
+            k0 = launches()
             sm.run_steps(a.steps)
+            k_launch += launches() - k0
             with torch.cuda.stream(stream):
                 e1.record(stream)
             torch.cuda.synchronize(dev)
@@ -452,7 +464,7 @@ def run_regimes(a, d: Dist):
                        "parallelism": f"replicas x{d.world}" if d.world > 1 else "single grid"},
             "regimes": out,
             "mostly_dry_vs_all_wet": out["mostly_dry"]["value"] / out["all_wet"]["value"],
-            "gpu_launches": 3 * a.steps * 2, "clocks": clk}
+            "gpu_launches": k_launch, "clocks": clk}
     if d.rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -485,9 +497,11 @@ def run_ensemble(a, d: Dist):
     d.barrier()
     clocks = ClockSampler(dev)
     clocks.start()
+    k_launch = launches()
     t0 = time.perf_counter()
     left = ens.run(a.steps)
     t1 = time.perf_counter()
+    k_launch = launches() - k_launch
     clk = clocks.stop()
     st1 = np.array([ens.info(k)["steps"] for k in range(len(mine))], dtype=np.float64)
     el = d.max(t1 - t0)
@@ -521,7 +535,7 @@ def run_ensemble(a, d: Dist):
             "loop_of_plain_solves": {"value": loop_rate, "unit": "cell-updates/s",
                                      "scenarios_timed": len(sub)},
             "speedup_vs_loop": (batched_rate / d.world) / loop_rate if loop_rate else None,
-            "gpu_launches": 4 * a.steps, "generation_s": gen_s,
+            "gpu_launches": k_launch, "generation_s": gen_s,
             "schedule": {"chosen": Ensemble.SCHEDULES.get(sched, "untuned"),
                          "tuning_ms_per_candidate": [float(x) for x in tune_ms],
                          "autotune_steps": 64},
@@ -555,21 +569,26 @@ def run_ensemble_complete(a, d: Dist, allscn, mine, gen_s):
     clocks.start()
     ens = Ensemble(mine, device=dev)
     torch.cuda.synchronize(dev)
+    k_batch = launches()
     t0 = time.perf_counter()
     left = ens.run()
     torch.cuda.synchronize(dev)
     batch_s = time.perf_counter() - t0
+    k_batch = launches() - k_batch
     info = [ens.info(k) for k in range(len(mine))]
     sched, _ = ens.schedule()
     ens.close()
     loop_s, loop_steps = [], []
+    k_loop = 0
     for s in mine:
         with workloads.simulation_for(s, device=dev) as sm:
             torch.cuda.synchronize(dev)
+            k0 = launches()
             ta = time.perf_counter()
             sm.run_until(s.t_end)
             torch.cuda.synchronize(dev)
             loop_s.append(time.perf_counter() - ta)
+            k_loop += launches() - k0
             loop_steps.append(sm.steps())
     clk = clocks.stop()
     steps = np.array([x["steps"] for x in info], dtype=np.float64)
@@ -579,7 +598,7 @@ def run_ensemble_complete(a, d: Dist, allscn, mine, gen_s):
                     "cell_updates": float(np.sum(cells * steps)),
                     "same_steps": bool(np.array_equal(steps, np.array(loop_steps))),
                     "steps": steps.tolist(), "sides": [s.shape[0] for s in mine],
-                    "loop_each": loop_s})
+                    "loop_each": loop_s, "k_batch": k_batch, "k_loop": k_loop})
     if d.rank != 0:
         return
     n_all = sum(x["n"] for x in tot)
@@ -602,7 +621,8 @@ def run_ensemble_complete(a, d: Dist, allscn, mine, gen_s):
             "batched_s": b_s, "scenarios_completed": sum(x["ok"] for x in tot),
             "unfinished": left,
             "loop_of_plain_solves": {"value": n_all / l_s, "unit": "solves/s", "seconds": l_s,
-                                     "steps_equal_batched": all(x["same_steps"] for x in tot)},
+                                     "steps_equal_batched": all(x["same_steps"] for x in tot),
+                                     "gpu_launches": sum(x["k_loop"] for x in tot)},
             "speedup_vs_loop": l_s / b_s,
             "cell_updates": sum(x["cell_updates"] for x in tot),
             "batched_cell_updates_per_s": sum(x["cell_updates"] for x in tot) / b_s,
@@ -610,7 +630,8 @@ def run_ensemble_complete(a, d: Dist, allscn, mine, gen_s):
                                    "max": int(st.max())},
             "loop_time_share_sides_le_256": float(each[small].sum() / max(each.sum(), 1e-30)),
             "schedule": Ensemble.SCHEDULES.get(sched, "untuned"),
-            "generation_s": gen_s, "gpu_launches": None, "clocks": clk}
+            "generation_s": gen_s, "gpu_launches": sum(x["k_batch"] for x in tot),
+            "clocks": clk}
     print(json.dumps(line), flush=True)
 
 
@@ -645,6 +666,7 @@ def run_adjoint(a, d: Dist):
         clocks = ClockSampler(dev)
         clocks.start()
         t_fwd, t_grad = [], []
+        k_launch = launches()
         for _ in range(reps):
             t0 = time.perf_counter()
             J, _, k_run = cal.run(s.manning)
@@ -653,6 +675,7 @@ def run_adjoint(a, d: Dist):
             t2 = time.perf_counter()
             t_fwd.append(t1 - t0)
             t_grad.append(t2 - t1)
+        k_launch = (launches() - k_launch) // max(reps, 1)
         clk = clocks.stop()
         f_s = d.max(statistics.median(t_fwd))
         g_s = d.max(statistics.median(t_grad))
@@ -725,7 +748,8 @@ def run_adjoint(a, d: Dist):
             "checks": {"dual_tangent_8_dirs_max_rel": max(dot_errs),
                        "central_fd_eps1e-6": fd_errs, "fd_by_horizon": by_horizon},
             # per misfit step: primal 5, replay 3, reverse 7 launches
-            "gpu_launches": int(k_run) * 15, "clocks": clk}
+            "gpu_launches": k_launch, "gpu_launches_per": "one forward solve + one gradient",
+            "clocks": clk}
     if d.rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -768,10 +792,13 @@ def run_lanes(a, d: Dist):
             torch.cuda.synchronize(dev)
 
             def timed(fn):
+                timed.k = launches()
                 t0 = time.perf_counter()
                 out = fn()
                 torch.cuda.synchronize(dev)
-                return time.perf_counter() - t0, out
+                el = time.perf_counter() - t0
+                timed.k = launches() - timed.k
+                return el, out
 
             f_s, _ = timed(lambda: cal.run(s.manning))
             g_s, (_, g) = timed(lambda: cal.gradient(s.manning))
@@ -784,6 +811,7 @@ def run_lanes(a, d: Dist):
                 # untimed first call at this lane count: lane buffers and graphs
                 cal.tangent_lanes(s.manning, dn=dn)
                 vm_s, (_, dJ) = timed(lambda: cal.tangent_lanes(s.manning, dn=dn))
+                vm_k = timed.k
                 same = bool(np.array_equal(np.array(sc), dJ))
                 zs = np.array([np.sum(g[:, zone == p]) for p in range(Pn)])
                 rel = float(np.max(np.abs(zs - dJ) / np.maximum(np.abs(dJ), 1e-300)))
@@ -791,7 +819,7 @@ def run_lanes(a, d: Dist):
                              "scalar_vs_forward": d.max(sc_s) / d.max(f_s),
                              "vector_vs_forward": d.max(vm_s) / d.max(f_s),
                              "vector_per_param": (d.max(vm_s) / d.max(f_s)) / Pn,
-                             "lanes_equal_scalar_runs": same,
+                             "lanes_equal_scalar_runs": same, "vector_gpu_launches": vm_k,
                              "adjoint_zone_sums_max_rel": rel})
                 t_all += sc_s + vm_s
         by_grid[f"{n_side}x{n_side}"] = {"cells": s.n_cells, "misfit_steps": K,
@@ -814,7 +842,7 @@ def run_lanes(a, d: Dist):
             "note": "steady state: each lane count runs once untimed (lane buffers, graph "
                     "capture) before its timed run; the scalar tangent's graphs are captured "
                     "in the warm-up",
-            "gpu_launches": int(a.calib_steps) * 5 * sum(counts) * 2, "clocks": clk}
+            "gpu_launches": p16["vector_gpu_launches"], "clocks": clk}
     if d.rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -850,8 +878,10 @@ def run_serve(a, d: Dist):
     d.barrier()
     clocks = ClockSampler(dev)
     clocks.start()
+    k_serve = launches()
     out = serve.serve_stream(mine, hbm_budget_bytes=150 << 30, device=dev, policy="srpt",
                              max_active_cells=a.max_active_cells)
+    k_serve = launches() - k_serve
     clk = clocks.stop()
     fifo = {"latencies": [], "makespan": float("nan")}
     if not a.no_fifo:
@@ -878,7 +908,7 @@ def run_serve(a, d: Dist):
     per_rank = d.gather({"served": list(out["latencies"]),
                          "fifo": list(fifo["latencies"]), "seq": lat,
                          "makespan": out["makespan"], "fifo_makespan": fifo["makespan"],
-                         "seq_end": t_free, "busy": float(sum(service))})
+                         "seq_end": t_free, "busy": float(sum(service)), "k": k_serve})
     if d.rank != 0:
         return
     cat = lambda k: np.concatenate([np.asarray(x[k], dtype=np.float64) for x in per_rank])  # noqa: E731
@@ -914,7 +944,7 @@ def run_serve(a, d: Dist):
             "payload_generation_s": gen_s,
             "sequential_plain": seq,
             "speedup_solves_per_s": out["solves_per_s"] / seq["solves_per_s"],
-            "gpu_launches": None, "clocks": clk}
+            "gpu_launches": sum(x["k"] for x in per_rank), "clocks": clk}
     print(json.dumps(line), flush=True)
 
 

@@ -24,6 +24,7 @@ PROTOTYPES = {
     "hf_last_error": (C.c_char_p, []),
     "hf_abi_version": (C.c_int, []),
     "hf_config_default": (None, [C.POINTER(abi.hf_config)]),
+    "hf_kernel_launches": (C.c_int, [C.POINTER(C.c_uint64)]),
     "hf_sim_create": (C.c_int, [C.POINTER(abi.hf_mesh_desc), _D, _D, _D,
                                 C.POINTER(abi.hf_config), C.c_int, C.POINTER(_VP)]),
     "hf_sim_create_aos": (C.c_int, [C.POINTER(abi.hf_mesh_desc), _D, C.POINTER(abi.hf_config),
@@ -134,3 +135,10 @@ def lib():
 
 def last_error() -> str:
     return lib().hf_last_error().decode()
+
+
+def kernel_launches() -> int:
+    """Kernels the library has launched in this process (hf_kernel_launches)."""
+    n = C.c_uint64()
+    lib().hf_kernel_launches(C.byref(n))
+    return n.value

@@ -733,7 +733,6 @@ __global__ void k_calib_rewind(Ctrl* c, const double* __restrict__ ts, long long
 }
 
 namespace {
-int cuda_rc(cudaError_t e) { return e == cudaSuccess ? 0 : -7; }
 int elem_grid(int64_t n) {
   int64_t g = (n + 255) / 256;
   if (g > 148 * 16) g = 148 * 16;
@@ -766,7 +765,7 @@ int launch_stage_adj(const StageArgs& a, const double* lam_h, const double* lam_
                      double* lam_un_hv, double* halo, int grid, void* stream) {
   AdjArgs j{lam_h, lam_hu, lam_hv, lam_un_h, lam_un_hu, lam_un_hv, halo};
   k_stage_adj<<<grid, NTHREADS, adj_smem_bytes(), (cudaStream_t)stream>>>(a, j);
-  return cuda_rc(cudaGetLastError());
+  return launched(stream);
 }
 
 int launch_adj_gather(int nr, int nc, int tiles_x, int tiles_y, const double* halo,
@@ -776,19 +775,19 @@ int launch_adj_gather(int nr, int nc, int tiles_x, int tiles_y, const double* ha
   const int64_t ncell = (int64_t)nr * nc;
   k_adj_gather<<<elem_grid(ncell), 256, 0, (cudaStream_t)stream>>>(
       nr, nc, tiles_x, tiles_y, halo, add_h, add_hu, add_hv, out_h, out_hu, out_hv, grad_n);
-  return cuda_rc(cudaGetLastError());
+  return launched(stream);
 }
 
 int launch_adj_seed(double* lam_h, const int64_t* cells, int n_gauges, const double* gauge_h,
                     const double* obs, void* stream) {
   if (n_gauges <= 0) return 0;
   k_adj_seed<<<1, 32, 0, (cudaStream_t)stream>>>(lam_h, cells, n_gauges, gauge_h, obs);
-  return cuda_rc(cudaGetLastError());
+  return launched(stream);
 }
 
 int launch_calib_pre(const Ctrl* c, double* dts, double* ts, long long cap, void* stream) {
   k_calib_pre<<<1, 32, 0, (cudaStream_t)stream>>>(c, dts, ts, cap);
-  return cuda_rc(cudaGetLastError());
+  return launched(stream);
 }
 
 int launch_calib_post(const Ctrl* c, const double* h, const double* dh, const int64_t* cells,
@@ -797,7 +796,7 @@ int launch_calib_post(const Ctrl* c, const double* h, const double* dh, const in
   if (n_gauges <= 0) return 0;
   k_calib_post<<<1, 128, 0, (cudaStream_t)stream>>>(c, h, dh, cells, n_gauges, gauge_h, gauge_dh,
                                                     cap, lanes, lane_stride);
-  return cuda_rc(cudaGetLastError());
+  return launched(stream);
 }
 
 int launch_calib_ckpt(const Ctrl* c, const double* h, const double* hu, const double* hv,
@@ -805,12 +804,12 @@ int launch_calib_ckpt(const Ctrl* c, const double* h, const double* hu, const do
                       void* stream) {
   k_calib_ckpt<<<elem_grid(ncell), 256, 0, (cudaStream_t)stream>>>(c, h, hu, hv, ckpt, every,
                                                                     cap, ncell);
-  return cuda_rc(cudaGetLastError());
+  return launched(stream);
 }
 
 int launch_calib_rewind(Ctrl* c, const double* ts, long long k, void* stream) {
   k_calib_rewind<<<1, 1, 0, (cudaStream_t)stream>>>(c, ts, k);
-  return cuda_rc(cudaGetLastError());
+  return launched(stream);
 }
 
 }  // namespace hf

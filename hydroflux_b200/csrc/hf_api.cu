@@ -417,7 +417,7 @@ void release_gauges(hf_sim* s) {
 
 void drop_graphs(hf_sim* s) {
   for (auto& g : s->graphs) {
-    if (g) cudaGraphExecDestroy(g);
+    if (g) graph_destroy(g);
     g = nullptr;
   }
 }
@@ -434,7 +434,7 @@ int build_graph(hf_sim* s, int which) {
     return rc;
   }
   HF_CUDA(e);
-  e = cudaGraphInstantiate(&s->graphs[which], graph, 0);
+  e = graph_instantiate(&s->graphs[which], graph);
   cudaGraphDestroy(graph);
   HF_CUDA(e);
   return HF_OK;
@@ -542,6 +542,12 @@ extern "C" {
 const char* hf_last_error(void) { return g_err.c_str(); }
 
 int hf_abi_version(void) { return HF_ABI_VERSION; }
+
+int hf_kernel_launches(uint64_t* count) {
+  if (!count) return fail(HF_ERR_INVALID_ARG, "null count");
+  *count = kernel_launch_count();
+  return HF_OK;
+}
 
 void hf_config_default(hf_config* cfg) {
   if (!cfg) return;
@@ -663,7 +669,7 @@ int hf_sim_step(hf_sim* s, double dt_cap, double* dt_out) {
   HF_TRY(build_graph(s, 0));
   HF_TRY(launch_set_step(s->d_ctrl, dt_cap, s->cfg.cfl, s->cfg.max_dt, s->cfg.check_finite,
                          s->stream));
-  HF_CUDA(cudaGraphLaunch(s->graphs[0], s->stream));
+  HF_CUDA(graph_launch(s->graphs[0], s->stream));
   HF_TRY(read_ctrl(s));
   HF_TRY(ctrl_status(s));
   s->last_dt = s->h_ctrl->dt;
@@ -688,7 +694,7 @@ int hf_sim_run_until(hf_sim* s, double t_target) {
     }
     const uint64_t steps_before = s->steps;
     HF_TRY(build_graph(s, which));
-    HF_CUDA(cudaGraphLaunch(s->graphs[which], s->stream));
+    HF_CUDA(graph_launch(s->graphs[which], s->stream));
     HF_TRY(read_ctrl(s));
     HF_TRY(ctrl_status(s));
     if (s->h_ctrl->dt > 0.0) s->last_dt = s->h_ctrl->dt;
@@ -712,7 +718,7 @@ int hf_sim_run_steps(hf_sim* s, uint64_t n_steps, double t_target) {
     const uint64_t k = left / (uint64_t)kChunk[which];
     if (k == 0) continue;
     HF_TRY(build_graph(s, which));
-    for (uint64_t r = 0; r < k; ++r) HF_CUDA(cudaGraphLaunch(s->graphs[which], s->stream));
+    for (uint64_t r = 0; r < k; ++r) HF_CUDA(graph_launch(s->graphs[which], s->stream));
     left -= k * (uint64_t)kChunk[which];
   }
   HF_TRY(read_ctrl(s));

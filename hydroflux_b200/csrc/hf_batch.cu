@@ -111,7 +111,7 @@ void destroy_batch(hf_batch* b) {
   if (b->stream) cudaStreamSynchronize(b->stream);
   for (auto& row : b->graphs)
     for (auto& ge : row)
-      if (ge) cudaGraphExecDestroy(ge);
+      if (ge) graph_destroy(ge);
   for (auto& f : b->forcing) {
     f.release_rain();
     f.release_src();
@@ -153,7 +153,7 @@ int build_batch_graph(hf_batch* b, int sched, int which) {
     return rc;
   }
   B_CUDA(e);
-  e = cudaGraphInstantiate(&b->graphs[sched][which], graph, 0);
+  e = graph_instantiate(&b->graphs[sched][which], graph);
   cudaGraphDestroy(graph);
   B_CUDA(e);
   return HF_OK;
@@ -216,7 +216,7 @@ int run_chunk(hf_batch* b, int sched, int which, int64_t* running, float* elapse
     B_CUDA(cudaEventCreate(&e1));
     B_CUDA(cudaEventRecord(e0, b->stream));
   }
-  B_CUDA(cudaGraphLaunch(b->graphs[sched][which], b->stream));
+  B_CUDA(graph_launch(b->graphs[sched][which], b->stream));
   if (elapsed_ms) B_CUDA(cudaEventRecord(e1, b->stream));
   B_CUDA(cudaMemcpyAsync(b->h_ctrl, b->d_ctrl, b->n * sizeof(Ctrl), cudaMemcpyDeviceToHost, b->stream));
   B_CUDA(cudaStreamSynchronize(b->stream));

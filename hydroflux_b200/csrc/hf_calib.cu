@@ -307,11 +307,11 @@ int forward_run(hf_calib* c, int mode, bool checkpoints, int64_t* n_run) {
         return rc;
       }
       C_CUDA(e);
-      e = cudaGraphInstantiate(&ge, graph, 0);
+      e = graph_instantiate(&ge, graph);
       cudaGraphDestroy(graph);
       C_CUDA(e);
     }
-    C_CUDA(cudaGraphLaunch(ge, c->stream));
+    C_CUDA(graph_launch(ge, c->stream));
     k += kFwdChunk[which];
     if (k < steps) {  // stop launching once the run has ended
       C_CUDA(cudaMemcpyAsync(c->h_ctrl, c->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost,
@@ -507,9 +507,9 @@ void destroy_calib(hf_calib* c) {
   for (auto& m : c->fgraphs)
     for (auto& k : m)
       for (auto& g : k)
-        if (g) cudaGraphExecDestroy(g);
+        if (g) graph_destroy(g);
   for (auto& g : c->lgraphs)
-    if (g) cudaGraphExecDestroy(g);
+    if (g) graph_destroy(g);
   c->forcing.release_rain();
   c->forcing.release_src();
   std::vector<void*> ptrs = {c->z,    c->n,    c->dn,   c->h0,   c->hu0,  c->hv0,  c->cells,
@@ -549,7 +549,7 @@ int upload_tangent_init(hf_calib* c, const double* dh0, const double* dhu0, cons
 void drop_lane_graphs(hf_calib* c) {
   for (auto& g : c->lgraphs)
     if (g) {
-      cudaGraphExecDestroy(g);
+      graph_destroy(g);
       g = nullptr;
     }
   c->lgraph_lanes = 0;
@@ -654,11 +654,11 @@ int forward_run_lanes(hf_calib* c, int lanes, int64_t* n_run) {
           return rc;
         }
         C_CUDA(e);
-        e = cudaGraphInstantiate(&ge, graph, 0);
+        e = graph_instantiate(&ge, graph);
         cudaGraphDestroy(graph);
         C_CUDA(e);
       }
-      C_CUDA(cudaGraphLaunch(ge, c->stream));
+      C_CUDA(graph_launch(ge, c->stream));
       k += kLaneChunk[which];
     } else {  // the last step of an odd count; k is even, so the values are in U
       C_TRY(enqueue_lane_step(vU, vA));

@@ -300,6 +300,17 @@ inline cudaError_t failed_call_error() {
   return l != cudaSuccess ? l : cudaErrorUnknown;
 }
 
+// Kernel launch accounting (hf_kernel_launches): every launcher ends with
+// launched(stream), which returns 0 or -7 like the launch check and counts
+// the launch unless the stream is being captured into a graph. Graphs are
+// instantiated, launched and destroyed through the three graph_* calls,
+// which count each launch as the kernel nodes of its graph.
+int launched(void* stream);
+cudaError_t graph_instantiate(cudaGraphExec_t* exec, cudaGraph_t graph);
+cudaError_t graph_launch(cudaGraphExec_t exec, cudaStream_t stream);
+void graph_destroy(cudaGraphExec_t exec);
+unsigned long long kernel_launch_count();
+
 // Device copies of one grid's forcing tables (host-side owner).
 struct ForcingHost {
   int n_rain = 0, n_src = 0;

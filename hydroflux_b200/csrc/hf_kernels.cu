@@ -17,7 +17,11 @@
 
 #include <type_traits>
 
+#include <atomic>
 #include <cstdio>
+#include <mutex>
+#include <unordered_map>
+#include <vector>
 
 #include "hf_device.cuh"
 #include "hf_internal.h"
@@ -697,6 +701,70 @@ int elem_grid(int64_t n) {
 
 cudaError_t last_launch_error() { return g_launch_error; }
 
+namespace {
+std::atomic<unsigned long long> g_kernel_launches{0};
+std::mutex g_graph_mu;
+std::unordered_map<cudaGraphExec_t, unsigned long long> g_graph_kernels;  // kernel nodes
+
+unsigned long long kernel_nodes(cudaGraph_t g) {
+  size_t n = 0;
+  if (cudaGraphGetNodes(g, nullptr, &n) != cudaSuccess || n == 0) return 0;
+  std::vector<cudaGraphNode_t> nodes(n);
+  if (cudaGraphGetNodes(g, nodes.data(), &n) != cudaSuccess) return 0;
+  unsigned long long k = 0;
+  for (size_t i = 0; i < n; ++i) {
+    cudaGraphNodeType t;
+    if (cudaGraphNodeGetType(nodes[i], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++k;
+  }
+  return k;
+}
+}  // namespace
+
+int launched(void* stream) {
+  const int rc = cuda_rc(cudaGetLastError());
+  if (rc != 0) return rc;
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing((cudaStream_t)stream, &st) != cudaSuccess) {
+    cudaGetLastError();  // the query failed: count the launch
+    st = cudaStreamCaptureStatusNone;
+  }
+  if (st == cudaStreamCaptureStatusNone) g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+  return 0;
+}
+
+cudaError_t graph_instantiate(cudaGraphExec_t* exec, cudaGraph_t graph) {
+  const cudaError_t e = cudaGraphInstantiate(exec, graph, 0);
+  if (e == cudaSuccess) {
+    const unsigned long long k = kernel_nodes(graph);
+    cudaGetLastError();  // a failed node query only leaves the count at 0
+    std::lock_guard<std::mutex> lock(g_graph_mu);
+    g_graph_kernels[*exec] = k;
+  }
+  return e;
+}
+
+cudaError_t graph_launch(cudaGraphExec_t exec, cudaStream_t stream) {
+  unsigned long long k = 0;
+  {
+    std::lock_guard<std::mutex> lock(g_graph_mu);
+    const auto it = g_graph_kernels.find(exec);
+    if (it != g_graph_kernels.end()) k = it->second;
+  }
+  const cudaError_t e = cudaGraphLaunch(exec, stream);
+  if (e == cudaSuccess) g_kernel_launches.fetch_add(k, std::memory_order_relaxed);
+  return e;
+}
+
+void graph_destroy(cudaGraphExec_t exec) {
+  {
+    std::lock_guard<std::mutex> lock(g_graph_mu);
+    g_graph_kernels.erase(exec);
+  }
+  cudaGraphExecDestroy(exec);
+}
+
+unsigned long long kernel_launch_count() { return g_kernel_launches.load(); }
+
 size_t stage_smem_bytes() { return sizeof(StageSmem); }
 
 int stage_grid_size(int tiles, int device) {
@@ -787,7 +855,7 @@ int strip_grid_size(int64_t nr, int64_t nc, int device) {
 
 int launch_stage_strip(const StageArgs& a, const StripMaps& m, int grid, void* stream) {
   k_stage_strip<<<grid, NTHREADS, kStripSmemBytes, (cudaStream_t)stream>>>(a, m);
-  return cuda_rc(cudaGetLastError());
+  return launched(stream);
 }
 
 int stage_dual_grid_size(int tiles, int device) {
@@ -817,12 +885,12 @@ int stage_dual_grid_size(int tiles, int device) {
 // stream capture).
 int launch_stage(const StageArgs& a, int grid, void* stream) {
   k_stage_pf<<<grid, NTHREADS, sizeof(StagePfSmem), (cudaStream_t)stream>>>(a);
-  return cuda_rc(cudaGetLastError());
+  return launched(stream);
 }
 
 int launch_finalize(const StageArgs& a, int grid, void* stream) {
   k_finalize<double><<<grid, NTHREADS, 0, (cudaStream_t)stream>>>(a);
-  return cuda_rc(cudaGetLastError());
+  return launched(stream);
 }
 
 // DualD (tangent) stage and finalize: value arrays in a.in_* / a.out_* /
@@ -830,77 +898,77 @@ int launch_finalize(const StageArgs& a, int grid, void* stream) {
 int launch_stage_dual(const StageArgs& a, int grid, void* stream, int lanes) {
   k_stage<DualD><<<dim3(grid, lanes), NTHREADS, sizeof(StageSmemT<DualD>),
                    (cudaStream_t)stream>>>(a);
-  return cuda_rc(cudaGetLastError());
+  return launched(stream);
 }
 
 int launch_finalize_dual(const StageArgs& a, int grid, void* stream, int lanes) {
   k_finalize<DualD><<<dim3(grid, lanes), NTHREADS, 0, (cudaStream_t)stream>>>(a);
-  return cuda_rc(cudaGetLastError());
+  return launched(stream);
 }
 
 int launch_stage_batch(const StageArgs* args, const int* tile_scn, const int* n_tiles, int grid,
                        void* stream, const int* tile_local, int* counter) {
   k_stage_batch<<<grid, NTHREADS, sizeof(StagePfSmem), (cudaStream_t)stream>>>(
       args, tile_scn, tile_local, n_tiles, counter);
-  return cuda_rc(cudaGetLastError());
+  return launched(stream);
 }
 
 int launch_cfl_batch(const StageArgs* args, const int* tile_scn, int first_tile, int last_tile,
                      int grid, void* stream) {
   if (last_tile <= first_tile) return 0;
   k_cfl_batch<<<grid, NTHREADS, 0, (cudaStream_t)stream>>>(args, tile_scn, first_tile, last_tile);
-  return cuda_rc(cudaGetLastError());
+  return launched(stream);
 }
 
 int launch_batch_control(Ctrl* ctrls, const StageArgs* args, int n, void* stream,
                          int* counters) {
   k_batch_control<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(ctrls, args, n, counters);
-  return cuda_rc(cudaGetLastError());
+  return launched(stream);
 }
 
 int launch_batch_commit(Ctrl* ctrls, int n, void* stream) {
   k_batch_commit<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(ctrls, n);
-  return cuda_rc(cudaGetLastError());
+  return launched(stream);
 }
 
 int launch_cfl(const StageArgs& a, int with_ghosts, int grid, void* stream) {
   k_cfl<<<grid, NTHREADS, 0, (cudaStream_t)stream>>>(a, with_ghosts);
-  return cuda_rc(cudaGetLastError());
+  return launched(stream);
 }
 
 int launch_control(Ctrl* ctrl, double dx, double dy, const ForcingDev& f, void* stream) {
   k_control<<<1, 256, 0, (cudaStream_t)stream>>>(ctrl, dx, dy, f);
-  return cuda_rc(cudaGetLastError());
+  return launched(stream);
 }
 
 int launch_gauges(const Ctrl* ctrl, const double* h, const GaugeDev& g, int init, void* stream) {
   k_gauges<<<1, 128, 0, (cudaStream_t)stream>>>(ctrl, h, g, init);
-  return cuda_rc(cudaGetLastError());
+  return launched(stream);
 }
 
 int launch_set_fixed(Ctrl* ctrl, double dt, void* stream) {
   k_set_fixed<<<1, 1, 0, (cudaStream_t)stream>>>(ctrl, dt);
-  return cuda_rc(cudaGetLastError());
+  return launched(stream);
 }
 
 int launch_set_step(Ctrl* ctrl, double dt_cap, double cfl, double max_dt, int check_finite,
                     void* stream) {
   k_set_step<<<1, 1, 0, (cudaStream_t)stream>>>(ctrl, dt_cap, cfl, max_dt, check_finite);
-  return cuda_rc(cudaGetLastError());
+  return launched(stream);
 }
 
 int launch_set_run(Ctrl* ctrl, double t_target, long long budget, double cfl, double max_dt,
                    int check_finite, int quiet_budget, void* stream) {
   k_set_run<<<1, 1, 0, (cudaStream_t)stream>>>(ctrl, t_target, budget, cfl, max_dt, check_finite,
                                                quiet_budget);
-  return cuda_rc(cudaGetLastError());
+  return launched(stream);
 }
 
 int launch_friction(int64_t ncell, const double* n, double* h, double* hu, double* hv, double dt,
                     double dry_tol, void* stream) {
   if (ncell <= 0) return 0;
   k_friction<<<elem_grid(ncell), 256, 0, (cudaStream_t)stream>>>(ncell, n, h, hu, hv, dt, dry_tol);
-  return cuda_rc(cudaGetLastError());
+  return launched(stream);
 }
 
 int launch_rain(int64_t ncell, double* h, double* hu, double* hv, double rate, double dt,
@@ -908,7 +976,7 @@ int launch_rain(int64_t ncell, double* h, double* hu, double* hv, double rate, d
   if (rate == 0.0 || ncell <= 0) return 0;  // source.rs:89-91
   const double dh = rate * dt;
   k_rain<<<elem_grid(ncell), 256, 0, (cudaStream_t)stream>>>(ncell, h, hu, hv, dh);
-  return cuda_rc(cudaGetLastError());
+  return launched(stream);
 }
 
 int launch_point_sources(int64_t nc, double* h, double* hu, double* hv, int n,
@@ -923,7 +991,7 @@ int launch_point_sources(int64_t nc, double* h, double* hu, double* hv, int n,
       pc.dh[k] = q[base + k] * dt / area;
     }
     k_point_sources<<<1, 32, 0, (cudaStream_t)stream>>>(pc, h, hu, hv);
-    int rc = cuda_rc(cudaGetLastError());
+    int rc = launched(stream);
     if (rc) return rc;
   }
   return 0;
@@ -933,20 +1001,20 @@ int launch_count_bad_manning(int64_t ncell, const double* n, unsigned long long*
                              void* stream) {
   if (ncell <= 0) return 0;
   k_count_bad_manning<<<elem_grid(ncell), 256, 0, (cudaStream_t)stream>>>(ncell, n, count);
-  return cuda_rc(cudaGetLastError());
+  return launched(stream);
 }
 
 int launch_relief(int64_t ncell, const double* h, const double* z, Ctrl* c, void* stream) {
   if (ncell <= 0) return 0;
   k_relief<<<elem_grid(ncell), 256, 0, (cudaStream_t)stream>>>(ncell, h, z, c);
-  return cuda_rc(cudaGetLastError());
+  return launched(stream);
 }
 
 int launch_hllc(int x_dir, int64_t n, const double* ul, const double* ur, double* out,
                 void* stream) {
   if (n <= 0) return 0;
   k_hllc<<<elem_grid(n), 256, 0, (cudaStream_t)stream>>>(x_dir, n, ul, ur, out);
-  return cuda_rc(cudaGetLastError());
+  return launched(stream);
 }
 
 }  // namespace hf

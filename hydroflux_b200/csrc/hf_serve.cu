@@ -107,7 +107,7 @@ void destroy_server(hf_server* v) {
   SGuard g(v->device);
   if (v->stream) cudaStreamSynchronize(v->stream);
   for (auto& ge : v->graphs)
-    if (ge) cudaGraphExecDestroy(ge);
+    if (ge) graph_destroy(ge);
   for (auto& s : v->slots) free_slot(s);
   for (void* p : {(void*)v->d_ctrl, (void*)v->d_args1, (void*)v->d_args2, (void*)v->d_tile_scn,
                   (void*)v->d_n_tiles, (void*)v->d_counters})
@@ -171,7 +171,7 @@ int build_serve_graph(hf_server* v, int which) {
     return rc;
   }
   S_CUDA(e);
-  e = cudaGraphInstantiate(&v->graphs[which], graph, 0);
+  e = graph_instantiate(&v->graphs[which], graph);
   cudaGraphDestroy(graph);
   S_CUDA(e);
   return HF_OK;
@@ -374,7 +374,7 @@ int hf_server_advance(hf_server* v, uint64_t n_batch_steps, int* n_finished) {
     long long before = 0;
     for (int k = 0; k < v->max_slots; ++k) before += v->h_ctrl[k].steps;
     S_TRY(build_serve_graph(v, which));
-    S_CUDA(cudaGraphLaunch(v->graphs[which], v->stream));
+    S_CUDA(graph_launch(v->graphs[which], v->stream));
     left -= (uint64_t)kServeChunk[which];
     int top = 0;  // control blocks past the highest used slot are idle
     for (int k = 0; k < v->max_slots; ++k)

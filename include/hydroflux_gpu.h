@@ -114,6 +114,11 @@ const char* hf_last_error(void);
 int hf_abi_version(void);
 /* Fills the reference defaults (SimulationConfig::default, sim.rs:67-77). */
 void hf_config_default(hf_config* cfg);
+/* Kernels this library has launched in this process, over every handle and
+ * thread: direct launches (not those captured into graphs) plus each kernel
+ * node of every graph launch. Read it before and after a region to count
+ * the region's kernels. HF_ERR_INVALID_ARG for a NULL count. */
+int hf_kernel_launches(uint64_t* count);
 
 /* ---------------------------------------------------------------------------
  * Simulation handle (replaces `Simulation`, sim.rs:119-245). Owns device

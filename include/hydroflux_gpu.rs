@@ -88,6 +88,7 @@ extern "C" {
     pub fn hf_last_error() -> *const c_char;
     pub fn hf_abi_version() -> c_int;
     pub fn hf_config_default(cfg: *mut HfConfig);
+    pub fn hf_kernel_launches(count: *mut u64) -> c_int;
     pub fn hf_sim_create(mesh: *const HfMeshDesc, h: *const f64, hu: *const f64, hv: *const f64,
                          cfg: *const HfConfig, device: c_int, out: *mut *mut HfSim) -> c_int;
     pub fn hf_sim_create_aos(mesh: *const HfMeshDesc, hhuhv: *const f64, cfg: *const HfConfig,

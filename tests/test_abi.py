@@ -85,6 +85,10 @@ def test_host_validation_without_gpu(libpath):
                            C.byref(abi.make_config(boundaries=q)), 0, C.byref(h))
     assert rc == abi.HF_ERR_INVALID_CONFIG
     assert lib.hf_sim_step(None, 1.0, None) == abi.HF_ERR_INVALID_ARG
+    # launch accounting: no GPU work was done, so nothing was launched
+    n = C.c_uint64(7)
+    assert lib.hf_kernel_launches(C.byref(n)) == abi.HF_OK and n.value == 0
+    assert lib.hf_kernel_launches(None) == abi.HF_ERR_INVALID_ARG
     assert lib.hf_release_cached_memory(-1) == abi.HF_ERR_INVALID_ARG
     # Mesh2D's spacing asserts (geometry.rs:59, 93) on the device-grid entry points
     for dx, dy in ((0.0, 1.0), (1.0, -1.0), (float("nan"), 1.0)):
