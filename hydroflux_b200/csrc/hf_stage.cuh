@@ -5,6 +5,8 @@
 // (friction, forcings) and the CFL reduction helpers.
 #pragma once
 
+#include <cstddef>
+
 #include <cuda_runtime.h>
 
 #include <type_traits>
@@ -28,6 +30,10 @@ constexpr int AW = TX + 2, AH = TY + 2, AN = AW * AH;       // alpha: rows [-1,T
 template <class T> struct StageSmemT {
   T h[R4N];
   double z[R3N];
+  // eta, u and v start 8 bytes past a 16-byte boundary: the pipelined stage
+  // stages z, hu and hv there with 16-byte copies of column pairs (even
+  // global column, odd halo index), which then land on 16-byte boundaries.
+  double pad_;
   T eta[R3N], u[R3N], v[R3N];
   T sxe[SXN], sxu[SXN], sxv[SXN];
   T sye[SYN], syu[SYN], syv[SYN];
@@ -171,6 +177,15 @@ __device__ __forceinline__ void cp_async8(double* smem, const double* gmem, bool
                "r"(bytes)
                : "memory");
 }
+// 16-byte copy of a column pair (both addresses 16-byte aligned); valid ==
+// false zero-fills.
+__device__ __forceinline__ void cp_async16(double* smem, const double* gmem, bool valid) {
+  const unsigned saddr = (unsigned)__cvta_generic_to_shared(smem);
+  const int bytes = valid ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(saddr), "l"(gmem),
+               "r"(bytes)
+               : "memory");
+}
 __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
@@ -180,17 +195,60 @@ __device__ __forceinline__ void cp_async_wait_all() {
 // which are dead once the faces are done).
 struct StagePfSmem {
   StageSmem s;
-  double hst[R4N];
+  alignas(16) double hst[R4N];
 };
+static_assert(R3W % 2 == 0 && R4W % 2 == 0 && TX % 2 == 0, "column pairs");
+static_assert(offsetof(StageSmem, h) % 16 == 0 && offsetof(StageSmem, eta) % 16 == 8 &&
+                  offsetof(StageSmem, u) % 16 == 8 && offsetof(StageSmem, v) % 16 == 8 &&
+                  offsetof(StagePfSmem, hst) % 16 == 0,
+              "16-byte staging copies");
 
 // Starts the copies of a tile's raw inputs: h (4-cell halo) into hst and z,
 // hu, hv (3-cell halo) into S.eta, S.u, S.v; cells outside the grid read as
 // zeros. Completed by cp_async_wait_all() and a barrier.
+//
+// With an even column count and 16-byte aligned fields, the copies move
+// column pairs (16 bytes; the halo's first column gj0 - 4 is even, so every
+// pair starts on an even global column and lies wholly inside or wholly
+// outside the grid). The 3-cell halo rows (columns gj0-3 .. gj0+TX+2) take
+// TX/2 + 1 pairs and one single column at each end. Otherwise every element
+// is copied alone.
 __device__ __forceinline__ void stage_prefetch(const StageArgs& A, StageSmem& S, double* hst,
                                                int tile) {
   const int nr = A.nr, nc = A.nc;
   const int tyi = tile / A.tiles_x;
   const int gi0 = tyi * TY, gj0 = (tile - tyi * A.tiles_x) * TX;
+  const uintptr_t any = (uintptr_t)A.in_h | (uintptr_t)A.z | (uintptr_t)A.in_hu |
+                        (uintptr_t)A.in_hv;
+  if (((nc & 1) | (int)(any & 15)) == 0) {
+    constexpr int PW = R4W / 2;  // pairs per 4-cell halo row
+    for (int k = threadIdx.x; k < R4H * PW; k += NTHREADS) {
+      const int r = k / PW, cc = 2 * (k - r * PW);
+      const int gi = gi0 + r - 4, gj = gj0 + cc - 4;
+      const bool real = gi >= 0 && gi < nr && gj >= 0 && gj < nc;
+      cp_async16(&hst[r * R4W + cc], A.in_h + (real ? (int64_t)gi * nc + gj : 0), real);
+    }
+    constexpr int NP = (R3W - 2) / 2;  // pairs per 3-cell halo row (columns 2 .. R3W-1)
+    for (int k = threadIdx.x; k < R3H * (NP + 2); k += NTHREADS) {
+      const int r3 = k / (NP + 2), j = k - r3 * (NP + 2);
+      const int cc = j < NP ? 2 + 2 * j : (j == NP ? 1 : R4W - 2);  // column of the 4-halo row
+      const int gi = gi0 + r3 - 3, gj = gj0 + cc - 4;
+      const bool real = gi >= 0 && gi < nr && gj >= 0 && gj < nc;
+      const int64_t g = real ? (int64_t)gi * nc + gj : 0;
+      const int k3 = r3 * R3W + (cc - 1);
+      if (j < NP) {
+        cp_async16(&S.eta[k3], A.z + g, real);
+        cp_async16(&S.u[k3], A.in_hu + g, real);
+        cp_async16(&S.v[k3], A.in_hv + g, real);
+      } else {
+        cp_async8(&S.eta[k3], A.z + g, real);
+        cp_async8(&S.u[k3], A.in_hu + g, real);
+        cp_async8(&S.v[k3], A.in_hv + g, real);
+      }
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    return;
+  }
   for (int k = threadIdx.x; k < R4N; k += NTHREADS) {
     const int r = k / R4W, cc = k - r * R4W;
     const int gi = gi0 + r - 4, gj = gj0 + cc - 4;

@@ -111,6 +111,41 @@ def test_step_parity_random(gpu, oracle, shape, bcname, integrator):
         assert exact_fraction(got, ref) == 1.0, f"step {it}: not bit-exact"
 
 
+@pytest.mark.parametrize("offset", [0, 1], ids=["aligned", "off16"])
+@pytest.mark.parametrize("shape", [(40, 70), (64, 96), (20, 67)], ids=lambda s: f"{s[0]}x{s[1]}")
+def test_step_parity_field_alignment(gpu, oracle, shape, offset):
+    """The pipelined stage stages its inputs with 16-byte copies of column
+    pairs when the column count is even and every field starts on a 16-byte
+    boundary, and element by element otherwise. Fields that start 8 bytes
+    into their buffers (offset 1) and odd column counts take the second
+    path; both give the oracle's bits."""
+    torch = pytest.importorskip("torch")
+    sim, step = gpu
+    nr, nc = shape
+    z, n, h, hu, hv = random_case(nr, nc, seed=nr * 7 + nc)
+    pairs = BC_SETS["mixed"]
+    bcs_c = abi.make_boundaries(*pairs)
+
+    def placed(a):
+        buf = torch.zeros(nr * nc + 2, dtype=torch.float64, device="cuda")
+        v = buf[offset:offset + nr * nc].view(nr, nc)
+        v.copy_(torch.as_tensor(a, dtype=torch.float64, device="cuda"))
+        assert v.data_ptr() % 16 == 8 * offset
+        return v
+
+    mesh = step.DeviceMesh(placed(z), 1.5, 0.75, placed(n))
+    assert mesh.bed.data_ptr() % 16 == 8 * offset
+    ws = step.StepWorkspace2D(nr, nc)
+    dh, dhu, dhv = placed(h), placed(hu), placed(hv)
+    ref = (h, hu, hv)
+    for it in range(4):
+        dt = min(oracle.cfl_time_step(z, 1.5, 0.75, *ref, 0.45, bcs=bcs_c, n=n), 0.05)
+        ref = oracle.ssprk2_step(z, 1.5, 0.75, *ref, bcs_c, dt, n)
+        step.ssprk2_step(dh, dhu, dhv, mesh, bcs_obj(sim, pairs), dt, ws)
+        got = to_host(dh, dhu, dhv)
+        assert exact_fraction(got, ref) == 1.0, f"step {it}: not bit-exact"
+
+
 @pytest.mark.parametrize("shape", [(1, 1), (7, 5), (128, 96)])
 def test_friction_rain_sources_parity(gpu, oracle, shape):
     sim, step = gpu
