@@ -49,7 +49,7 @@ def parse():
     p.add_argument("--cpu-steps", type=int, default=2, help="oracle steps in the CPU baseline")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--stage-kernel", default="auto", choices=["auto", "tile", "strip"],
+    p.add_argument("--stage-kernel", default="auto", choices=["auto", "tile", "tile32", "strip"],
                    help="valley: the stage kernel (hf_sim_set_stage_kernel; bit-identical)")
     p.add_argument("--workload", default="valley", choices=["valley", "ensemble", "adjoint",
                                                             "serve", "lanes", "regimes"],
@@ -145,6 +145,10 @@ def measured_peaks():
         return float(d["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+# The stage kernel in use, as named in the committed ncu summaries.
+KERNEL_NAMES = {"tile": "k_stage_pf/32x8", "tile32": "k_stage_pf/32x32", "strip": "k_stage_strip"}
 
 
 def profiled_figure(kernel, key):
@@ -275,7 +279,7 @@ def run_ours(a, d: Dist):
     bytes_per_launch = ALG_BYTES_PER_CELL_UPDATE / STAGE_LAUNCHES_PER_STEP * cells
     achieved_gbs = bytes_per_launch / avg_stage_s / 1e9
     peak, peak_kind = measured_peaks()
-    kernel = "k_stage_strip" if sm.stage_kernel() == "strip" else "k_stage_pf"
+    kernel = KERNEL_NAMES[sm.stage_kernel()]
     traffic_per_cell = profiled_traffic(kernel)
     sm.close()
 
@@ -451,7 +455,7 @@ def run_regimes(a, d: Dist):
                    "sample": "1 step of the same state, CPU oracle, 1 thread"}
         out[kind] = {"value": d.world * scn.n_cells * a.steps / (ms / 1e3), "unit": UNIT,
                      "ms_per_step": ms / a.steps, "wet_fraction": round(wet, 4),
-                     "stage_kernel": f"k_stage_{kernel}" if kernel == "strip" else "k_stage_pf",
+                     "stage_kernel": KERNEL_NAMES[kernel],
                      "cpu_baseline": cpu}
     clk = clocks.stop()
     line = {"metric": "cell-updates/s (mostly dry)", "value": out["mostly_dry"]["value"],

@@ -26,6 +26,7 @@
 #include "hf_stage.cuh"
 
 namespace hf {
+inline namespace HF_GEOM {
 
 namespace {
 
@@ -812,4 +813,5 @@ int launch_calib_rewind(Ctrl* c, const double* ts, long long k, void* stream) {
   return launched(stream);
 }
 
+}  // namespace HF_GEOM
 }  // namespace hf

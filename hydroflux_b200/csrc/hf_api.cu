@@ -191,15 +191,16 @@ void ForcingHost::release_rain() {
 
 void ForcingHost::release_src() {
   for (void* p : {(void*)d_row, (void*)d_col, (void*)d_off, (void*)d_st, (void*)d_sq,
-                  (void*)d_tile_start, (void*)d_tile_order, (void*)d_blk_start,
-                  (void*)d_blk_order, (void*)d_dh})
+                  (void*)d_tile_start[0], (void*)d_tile_order[0], (void*)d_tile_start[1],
+                  (void*)d_tile_order[1], (void*)d_blk_start, (void*)d_blk_order, (void*)d_dh})
     dfree(p);
-  d_row = d_col = d_off = d_tile_start = d_tile_order = d_blk_start = d_blk_order = nullptr;
+  d_row = d_col = d_off = d_blk_start = d_blk_order = nullptr;
+  d_tile_start[0] = d_tile_order[0] = d_tile_start[1] = d_tile_order[1] = nullptr;
   d_st = d_sq = d_dh = nullptr;
   n_src = 0;
 }
 
-ForcingDev ForcingHost::dev() const {
+ForcingDev ForcingHost::dev(int geom) const {
   ForcingDev f;
   f.n_rain = n_rain;
   f.n_src = n_src;
@@ -210,8 +211,8 @@ ForcingDev ForcingHost::dev() const {
   f.src_off = d_off;
   f.src_t = d_st;
   f.src_q = d_sq;
-  f.tile_start = d_tile_start;
-  f.tile_order = d_tile_order;
+  f.tile_start = d_tile_start[geom];
+  f.tile_order = d_tile_order[geom];
   f.blk_start = d_blk_start;
   f.blk_order = d_blk_order;
   f.src_dh = d_dh;
@@ -235,9 +236,9 @@ int hf::forcing_set_rain(ForcingHost& f, int64_t n_points, const double* t, cons
   return HF_OK;
 }
 
-int hf::forcing_set_sources(ForcingHost& f, int64_t nr, int64_t nc, int tiles_x, int tiles_y,
-                            int64_t n_sources, const int64_t* rows, const int64_t* cols,
-                            const int64_t* offsets, const double* t, const double* q) {
+int hf::forcing_set_sources(ForcingHost& f, int64_t nr, int64_t nc, int64_t n_sources,
+                            const int64_t* rows, const int64_t* cols, const int64_t* offsets,
+                            const double* t, const double* q) {
   if (n_sources < 0) return fail(HF_ERR_INVALID_ARG, "bad point sources");
   if (n_sources > 0 && (!rows || !cols || !offsets || !t || !q))
     return fail(HF_ERR_INVALID_ARG, "null point-source arrays");
@@ -259,8 +260,9 @@ int hf::forcing_set_sources(ForcingHost& f, int64_t nr, int64_t nc, int tiles_x,
     c[k] = (int)cols[k];
   }
   for (int k = 0; k <= ns; ++k) off[k] = (int)offsets[k];
-  // Bucket the sources by stage tile and by strip block, keeping their order
-  // within a bucket (repeated cells accumulate in the caller's order).
+  // Bucket the sources by the stage tiles of each geometry and by strip
+  // block, keeping their order within a bucket (repeated cells accumulate in
+  // the caller's order).
   auto bucket = [&](int nbuckets, auto key, std::vector<int>& start, std::vector<int>& order) {
     start.assign(nbuckets + 1, 0);
     order.assign(ns, 0);
@@ -269,9 +271,15 @@ int hf::forcing_set_sources(ForcingHost& f, int64_t nr, int64_t nc, int tiles_x,
     std::vector<int> fill(start.begin(), start.end() - 1);
     for (int k = 0; k < ns; ++k) order[fill[key(k)]++] = k;
   };
-  const int ntiles = tiles_x * tiles_y;
-  std::vector<int> start, order, bstart, border;
-  bucket(ntiles, [&](int k) { return (r[k] / TY) * tiles_x + c[k] / TX; }, start, order);
+  std::vector<int> start[2], order[2], bstart, border;
+  const int tiles_x = tiles_along(nc, TX);
+  int ntiles[2];
+  for (int g = 0; g < 2; ++g) {
+    const int th = kGeomTileH[g];
+    ntiles[g] = tiles_x * tiles_along(nr, th);
+    bucket(ntiles[g], [&](int k) { return (r[k] / th) * tiles_x + c[k] / TX; }, start[g],
+           order[g]);
+  }
   const int nb = strip_blocks(nr), nblk = strip_count(nc) * nb;
   bucket(nblk, [&](int k) { return (c[k] / TX) * nb + r[k] / STRIP_ROWS; }, bstart, border);
   HF_TRY(dalloc(&f.d_row, ns));
@@ -279,8 +287,10 @@ int hf::forcing_set_sources(ForcingHost& f, int64_t nr, int64_t nc, int tiles_x,
   HF_TRY(dalloc(&f.d_off, ns + 1));
   HF_TRY(dalloc(&f.d_st, npts));
   HF_TRY(dalloc(&f.d_sq, npts));
-  HF_TRY(dalloc(&f.d_tile_start, ntiles + 1));
-  HF_TRY(dalloc(&f.d_tile_order, ns));
+  for (int g = 0; g < 2; ++g) {
+    HF_TRY(dalloc(&f.d_tile_start[g], ntiles[g] + 1));
+    HF_TRY(dalloc(&f.d_tile_order[g], ns));
+  }
   HF_TRY(dalloc(&f.d_blk_start, nblk + 1));
   HF_TRY(dalloc(&f.d_blk_order, ns));
   HF_TRY(dalloc(&f.d_dh, ns));
@@ -289,9 +299,12 @@ int hf::forcing_set_sources(ForcingHost& f, int64_t nr, int64_t nc, int tiles_x,
   HF_CUDA(cudaMemcpy(f.d_off, off.data(), (ns + 1) * sizeof(int), cudaMemcpyHostToDevice));
   HF_CUDA(cudaMemcpy(f.d_st, t, npts * sizeof(double), cudaMemcpyHostToDevice));
   HF_CUDA(cudaMemcpy(f.d_sq, q, npts * sizeof(double), cudaMemcpyHostToDevice));
-  HF_CUDA(cudaMemcpy(f.d_tile_start, start.data(), (ntiles + 1) * sizeof(int),
-                     cudaMemcpyHostToDevice));
-  HF_CUDA(cudaMemcpy(f.d_tile_order, order.data(), ns * sizeof(int), cudaMemcpyHostToDevice));
+  for (int g = 0; g < 2; ++g) {
+    HF_CUDA(cudaMemcpy(f.d_tile_start[g], start[g].data(), (ntiles[g] + 1) * sizeof(int),
+                       cudaMemcpyHostToDevice));
+    HF_CUDA(cudaMemcpy(f.d_tile_order[g], order[g].data(), ns * sizeof(int),
+                       cudaMemcpyHostToDevice));
+  }
   HF_CUDA(cudaMemcpy(f.d_blk_start, bstart.data(), (nblk + 1) * sizeof(int),
                      cudaMemcpyHostToDevice));
   HF_CUDA(cudaMemcpy(f.d_blk_order, border.data(), ns * sizeof(int), cudaMemcpyHostToDevice));
@@ -315,8 +328,13 @@ struct hf_sim {
   ForcingHost forcing;
   GaugeDev gauge{};  // n == 0: no gauges
   cudaGraphExec_t graphs[3] = {nullptr, nullptr, nullptr};
-  // Stage kernel: HF_STAGE_TILE (k_stage_pf) or HF_STAGE_STRIP (k_stage_strip,
-  // with the TMA descriptors of stage 1's and stage 2's inputs).
+  // Tile geometry of the tile-shaped kernels (kGeomSmall / kGeomLarge) and
+  // its entry points; tiles_x, tiles_y and grid are in its tiles.
+  int geom = kGeomSmall;
+  const GeomOps* ops = nullptr;
+  // Stage kernel: HF_STAGE_TILE / HF_STAGE_TILE32 (k_stage_pf of the 32 x 8
+  // or 32 x 32 geometry) or HF_STAGE_STRIP (k_stage_strip, with the TMA
+  // descriptors of stage 1's and stage 2's inputs).
   int stage_kind = HF_STAGE_TILE;
   int strip_grid = 0;
   StripMaps maps[2];
@@ -347,7 +365,7 @@ StageArgs stage_args(const hf_sim* s, bool second) {
   a.bc = to_bcdev(s->cfg.boundaries);
   a.ctrl = s->d_ctrl;
   a.dry_tol = s->cfg.friction_dry_tol;
-  a.f = s->forcing.dev();
+  a.f = s->forcing.dev(s->geom);
   const bool ssp = s->cfg.integrator == HF_SSPRK2;
   if (!second) {  // U -> U1
     a.in_h = s->d_h; a.in_hu = s->d_hu; a.in_hv = s->d_hv;
@@ -371,15 +389,30 @@ int launch_sim_stage(hf_sim* s, bool second) {
   const StageArgs a = stage_args(s, second);
   if (s->stage_kind == HF_STAGE_STRIP)
     return launch_stage_strip(a, s->maps[second ? 1 : 0], s->strip_grid, s->stream);
-  return launch_stage(a, s->grid, s->stream);
+  return s->ops->stage(a, s->grid, s->stream);
+}
+
+// Puts the tile-shaped kernels of the simulation on geometry `geom`.
+void set_geom(hf_sim* s, int geom) {
+  s->geom = geom;
+  s->ops = &geom_ops(geom);
+  s->tiles_x = tiles_along(s->nc, TX);
+  s->tiles_y = tiles_along(s->nr, s->ops->tile_h);
+  s->grid = s->ops->grid_size(s->tiles_x * s->tiles_y, s->device);
 }
 
 // Picks the stage kernel: the strip kernel where it is asked for and its TMA
-// descriptors can be made, else the tile kernel (also for `kind` auto: on
-// B200 the tile kernel measured faster on wet grids and as fast on mostly
-// dry ones).
+// descriptors can be made, else the tile kernel of the geometry asked for;
+// auto takes the tile kernel of the grid's geometry (geom_for: on B200 the
+// tile kernel measured faster than the strip kernel on wet grids and as fast
+// on mostly dry ones). The strip kernel's grids keep the 32 x 8 geometry for
+// the CFL reduction and the forward-Euler finalize.
 int choose_stage_kernel(hf_sim* s, int kind) {
-  s->stage_kind = HF_STAGE_TILE;
+  const int geom = kind == HF_STAGE_TILE32   ? kGeomLarge
+                   : kind == HF_STAGE_AUTO ? geom_for(s->nr, s->nc)
+                                           : kGeomSmall;
+  set_geom(s, geom);
+  s->stage_kind = geom == kGeomLarge ? HF_STAGE_TILE32 : HF_STAGE_TILE;
   if (kind != HF_STAGE_STRIP) return HF_OK;
   int g = strip_grid_size(s->nr, s->nc, s->device);
   if (g == 0) {  // a small grid: one CTA per block at most
@@ -388,21 +421,23 @@ int choose_stage_kernel(hf_sim* s, int kind) {
     if (nq < g) g = (int)nq;
   }
   if (!(g > 0 && strip_maps(stage_args(s, false), s->maps[0]) &&
-        strip_maps(stage_args(s, true), s->maps[1])))
+        strip_maps(stage_args(s, true), s->maps[1]))) {
+    choose_stage_kernel(s, HF_STAGE_AUTO);
     return fail(HF_ERR_UNSUPPORTED,
                 "the strip stage kernel needs an even column count and 16-byte aligned fields");
+  }
   s->stage_kind = HF_STAGE_STRIP;
   s->strip_grid = g;
   return HF_OK;
 }
 
 int enqueue_step(hf_sim* s) {
-  HF_TRY(launch_control(s->d_ctrl, s->dx, s->dy, s->forcing.dev(), s->stream));
+  HF_TRY(launch_control(s->d_ctrl, s->dx, s->dy, s->forcing.dev(s->geom), s->stream));
   HF_TRY(launch_sim_stage(s, false));
   if (s->cfg.integrator == HF_SSPRK2)
     HF_TRY(launch_sim_stage(s, true));
   else
-    HF_TRY(launch_finalize(stage_args(s, true), s->grid, s->stream));
+    HF_TRY(s->ops->finalize(stage_args(s, true), s->grid, s->stream));
   if (s->gauge.n > 0) HF_TRY(launch_gauges(s->d_ctrl, s->d_h, s->gauge, 0, s->stream));
   return HF_OK;
 }
@@ -444,7 +479,7 @@ int refresh_cfl(hf_sim* s) {
   if (!s->cfl_dirty) return HF_OK;
   HF_CUDA(cudaMemsetAsync(&s->d_ctrl->sx_bits, 0, 3 * sizeof(unsigned long long), s->stream));
   StageArgs a = stage_args(s, false);
-  HF_TRY(launch_cfl(a, 1, s->grid, s->stream));
+  HF_TRY(s->ops->cfl(a, 1, s->grid, s->stream));
   s->cfl_dirty = false;
   return HF_OK;
 }
@@ -588,9 +623,7 @@ int hf_sim_create(const hf_mesh_desc* mesh, const double* h, const double* hu, c
   s->dx = mesh->dx;
   s->dy = mesh->dy;
   s->cfg = *cfg;
-  s->tiles_x = (int)((s->nc + TX - 1) / TX);
-  s->tiles_y = (int)((s->nr + TY - 1) / TY);
-  s->grid = stage_grid_size(s->tiles_x * s->tiles_y, device);
+  set_geom(s, geom_for(s->nr, s->nc));
   int rc = HF_OK;
   auto done = [&](int code) {
     if (code != HF_OK) destroy_sim(s);
@@ -744,13 +777,13 @@ int hf_sim_run_steps_timed(hf_sim* s, uint64_t n_steps, double t_target, double*
   for (auto& e : ev) HF_CUDA(cudaEventCreate(&e));
   int rc = HF_OK;
   for (uint64_t k = 0; k < n_steps && rc == HF_OK; ++k) {
-    rc = launch_control(s->d_ctrl, s->dx, s->dy, s->forcing.dev(), s->stream);
+    rc = launch_control(s->d_ctrl, s->dx, s->dy, s->forcing.dev(s->geom), s->stream);
     if (rc) break;
     cudaEventRecord(ev[3 * k], s->stream);
     rc = launch_sim_stage(s, false);
     if (rc) break;
     cudaEventRecord(ev[3 * k + 1], s->stream);
-    rc = ssp ? launch_sim_stage(s, true) : launch_finalize(stage_args(s, true), s->grid, s->stream);
+    rc = ssp ? launch_sim_stage(s, true) : s->ops->finalize(stage_args(s, true), s->grid, s->stream);
     cudaEventRecord(ev[3 * k + 2], s->stream);
     if (rc == HF_OK && s->gauge.n > 0)
       rc = launch_gauges(s->d_ctrl, s->d_h, s->gauge, 0, s->stream);
@@ -858,7 +891,8 @@ int hf_sim_set_boundaries(hf_sim* s, const hf_boundaries* bcs) {
 
 int hf_sim_set_stage_kernel(hf_sim* s, int kind) {
   if (!s) return fail(HF_ERR_INVALID_ARG, "null handle");
-  if (kind != HF_STAGE_AUTO && kind != HF_STAGE_TILE && kind != HF_STAGE_STRIP)
+  if (kind != HF_STAGE_AUTO && kind != HF_STAGE_TILE && kind != HF_STAGE_STRIP &&
+      kind != HF_STAGE_TILE32)
     return fail(HF_ERR_INVALID_ARG, "unknown stage kernel");
   DeviceGuard guard(s->device);
   cudaStreamSynchronize(s->stream);
@@ -904,7 +938,7 @@ int hf_sim_set_point_sources(hf_sim* s, int64_t n_sources, const int64_t* rows,
   DeviceGuard guard(s->device);
   cudaStreamSynchronize(s->stream);
   drop_graphs(s);
-  return forcing_set_sources(s->forcing, s->nr, s->nc, s->tiles_x, s->tiles_y, n_sources, rows,
+  return forcing_set_sources(s->forcing, s->nr, s->nc, n_sources, rows,
                              cols, offsets, t, q);
 }
 
@@ -1080,13 +1114,15 @@ int check_grid(const hf_grid* g, hf_workspace* w) {
   return HF_OK;
 }
 
-StageArgs ws_args(const hf_grid* g, const hf_boundaries& bcs, hf_workspace* w) {
+// Stage arguments of a device grid in the tiles of geometry `o`.
+StageArgs ws_args(const hf_grid* g, const hf_boundaries& bcs, hf_workspace* w,
+                  const GeomOps& o) {
   StageArgs a;
   std::memset(&a, 0, sizeof a);
   a.nr = (int)g->n_rows;
   a.nc = (int)g->n_cols;
-  a.tiles_x = (int)((g->n_cols + TX - 1) / TX);
-  a.tiles_y = (int)((g->n_rows + TY - 1) / TY);
+  a.tiles_x = tiles_along(g->n_cols, TX);
+  a.tiles_y = tiles_along(g->n_rows, o.tile_h);
   a.dx = g->dx;
   a.dy = g->dy;
   a.rx = hfa::make_recip(a.dx);
@@ -1111,13 +1147,14 @@ int euler_like(const hf_grid* grid, double* h, double* hu, double* hv, const hf_
   const hf_boundaries b = bcs ? *bcs : transmissive();
   HF_TRY(check_bcs(b, grid->n_rows, grid->n_cols));
   DeviceGuard guard(w->device);
-  StageArgs a = ws_args(grid, b, w);
-  const int gsz = stage_grid_size(a.tiles_x * a.tiles_y, w->device);
+  const GeomOps& o = geom_ops(geom_for(grid->n_rows, grid->n_cols));
+  StageArgs a = ws_args(grid, b, w, o);
+  const int gsz = o.grid_size(a.tiles_x * a.tiles_y, w->device);
   HF_TRY(launch_set_fixed(w->d_ctrl, dt, stream));
   a.in_h = h; a.in_hu = hu; a.in_hv = hv;
   a.out_h = w->d_h1; a.out_hu = w->d_hu1; a.out_hv = w->d_hv1;
   a.un_h = h; a.un_hu = hu; a.un_hv = hv;
-  HF_TRY(launch_stage(a, gsz, stream));
+  HF_TRY(o.stage(a, gsz, stream));
   const size_t bytes = (size_t)(grid->n_rows * grid->n_cols) * sizeof(double);
   if (!ssp) {
     cudaStream_t st = (cudaStream_t)stream;
@@ -1129,7 +1166,7 @@ int euler_like(const hf_grid* grid, double* h, double* hu, double* hv, const hf_
   a.in_h = w->d_h1; a.in_hu = w->d_hu1; a.in_hv = w->d_hv1;
   a.out_h = h; a.out_hu = hu; a.out_hv = hv;
   a.combine = 1;
-  HF_TRY(launch_stage(a, gsz, stream));
+  HF_TRY(o.stage(a, gsz, stream));
   return HF_OK;
 }
 
@@ -1146,10 +1183,11 @@ int hf_cfl_time_step(const hf_grid* grid, const double* h, const double* hu, con
   }
   DeviceGuard guard(w->device);
   cudaStream_t st = (cudaStream_t)stream;
-  StageArgs a = ws_args(grid, bcs ? *bcs : transmissive(), w);
+  const GeomOps& o = geom_ops(geom_for(grid->n_rows, grid->n_cols));
+  StageArgs a = ws_args(grid, bcs ? *bcs : transmissive(), w, o);
   a.in_h = h; a.in_hu = hu; a.in_hv = hv;
   HF_CUDA(cudaMemsetAsync(&w->d_ctrl->sx_bits, 0, 3 * sizeof(unsigned long long), st));
-  HF_TRY(launch_cfl(a, bcs ? 1 : 0, stage_grid_size(a.tiles_x * a.tiles_y, w->device), stream));
+  HF_TRY(o.cfl(a, bcs ? 1 : 0, o.grid_size(a.tiles_x * a.tiles_y, w->device), stream));
   HF_CUDA(cudaMemcpyAsync(w->h_ctrl, w->d_ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
   HF_CUDA(cudaStreamSynchronize(st));
   double sx, sy;

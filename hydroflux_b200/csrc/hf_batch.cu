@@ -72,6 +72,11 @@ constexpr int kSchedules = 4;  // bit 0: dynamic; bit 1: largest scenarios first
 struct hf_batch {
   int device = 0;
   cudaStream_t stream = nullptr;
+  // Tile geometry of the batched kernels: 32 x 32 once the ensemble has
+  // kLargeTilesMin such tiles (the tiles of all scenarios fill the GPU),
+  // else 32 x 8.
+  int geom = kGeomSmall;
+  const GeomOps* ops = nullptr;
   int n = 0;
   int64_t total_cells = 0;
   int total_tiles = 0;
@@ -133,9 +138,9 @@ int enqueue_batch_step(hf_batch* b, int sched) {
   int* c2 = dynamic ? b->d_counters + 1 : nullptr;
   if (launch_batch_control(b->d_ctrl, b->d_args1, b->n, b->stream, dynamic ? b->d_counters : nullptr))
     return bcuda(failed_call_error(), "control");
-  if (launch_stage_batch(b->d_args1, scn, b->d_n_tiles, b->grid, b->stream, local, c1))
+  if (b->ops->stage_batch(b->d_args1, scn, b->d_n_tiles, b->grid, b->stream, local, c1))
     return bcuda(failed_call_error(), "stage 1");
-  if (launch_stage_batch(b->d_args2, scn, b->d_n_tiles, b->grid, b->stream, local, c2))
+  if (b->ops->stage_batch(b->d_args2, scn, b->d_n_tiles, b->grid, b->stream, local, c2))
     return bcuda(failed_call_error(), "stage 2");
   if (launch_batch_commit(b->d_ctrl, b->n, b->stream)) return bcuda(failed_call_error(), "commit");
   return HF_OK;
@@ -243,7 +248,7 @@ int hf_batch_create(int64_t n_scenarios, const hf_scenario_desc* sc, int device,
   if (!out || !sc || n_scenarios <= 0) return bfail(HF_ERR_INVALID_ARG, "bad arguments");
   if (n_scenarios > (1 << 24)) return bfail(HF_ERR_INVALID_ARG, "too many scenarios");
   *out = nullptr;
-  int64_t total = 0, tiles = 0;
+  int64_t total = 0, tiles = 0, tiles_large = 0;
   for (int64_t k = 0; k < n_scenarios; ++k) {
     const hf_scenario_desc& d = sc[k];
     if (!d.mesh.bed || !d.h || !d.hu || !d.hv) return bfail(HF_ERR_INVALID_ARG, "null scenario arrays");
@@ -261,8 +266,12 @@ int hf_batch_create(int64_t n_scenarios, const hf_scenario_desc* sc, int device,
       return bfail(HF_ERR_INVALID_ARG, "Manning n must be non-negative");
     }
     total += nc;
-    tiles += ((d.mesh.n_cols + TX - 1) / TX) * ((d.mesh.n_rows + TY - 1) / TY);
+    const int64_t tx = tiles_along(d.mesh.n_cols, TX);
+    tiles += tx * tiles_along(d.mesh.n_rows, kGeomTileH[kGeomSmall]);
+    tiles_large += tx * tiles_along(d.mesh.n_rows, kGeomTileH[kGeomLarge]);
   }
+  const int geom = tiles_large >= kLargeTilesMin ? kGeomLarge : kGeomSmall;
+  if (geom == kGeomLarge) tiles = tiles_large;
   if (tiles > INT_MAX / 2) return bfail(HF_ERR_INVALID_ARG, "ensemble too large");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
@@ -279,7 +288,9 @@ int hf_batch_create(int64_t n_scenarios, const hf_scenario_desc* sc, int device,
   b->n = (int)n_scenarios;
   b->total_cells = total;
   b->total_tiles = (int)tiles;
-  b->grid = stage_grid_size(b->total_tiles, device);
+  b->geom = geom;
+  b->ops = &geom_ops(geom);
+  b->grid = b->ops->grid_size(b->total_tiles, device);
   b->forcing.resize(b->n);
   if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
     return done(bcuda(failed_call_error(), "cudaStreamCreate"));
@@ -325,10 +336,10 @@ int hf_batch_create(int64_t n_scenarios, const hf_scenario_desc* sc, int device,
       if (cudaMemcpy(b->nman + o, nn.data(), bytes, cudaMemcpyHostToDevice) != cudaSuccess)
         return done(bcuda(failed_call_error(), "upload manning"));
     }
-    const int tx = (int)((nc + TX - 1) / TX), ty = (int)((nr + TY - 1) / TY);
+    const int tx = tiles_along(nc, TX), ty = tiles_along(nr, b->ops->tile_h);
     int rc = forcing_set_rain(b->forcing[s], d.n_rain, d.rain_t, d.rain_rate);
     if (rc == HF_OK)
-      rc = forcing_set_sources(b->forcing[s], nr, nc, tx, ty, d.n_sources, d.src_rows, d.src_cols,
+      rc = forcing_set_sources(b->forcing[s], nr, nc, d.n_sources, d.src_rows, d.src_cols,
                                d.src_offsets, d.src_t, d.src_q);
     if (rc != HF_OK) return done(rc);
     Ctrl& c = b->h_ctrl[s];
@@ -354,7 +365,7 @@ int hf_batch_create(int64_t n_scenarios, const hf_scenario_desc* sc, int device,
     x.bc = boundaries_dev(d.cfg.boundaries);
     x.ctrl = b->d_ctrl + s;
     x.dry_tol = d.cfg.friction_dry_tol;
-    x.f = b->forcing[s].dev();
+    x.f = b->forcing[s].dev(b->geom);
     StageArgs y = x;
     x.in_h = b->h + o; x.in_hu = b->hu + o; x.in_hv = b->hv + o;
     x.out_h = b->h1 + o; x.out_hu = b->hu1 + o; x.out_hv = b->hv1 + o;
@@ -398,7 +409,7 @@ int hf_batch_create(int64_t n_scenarios, const hf_scenario_desc* sc, int device,
       cudaMemcpy(b->d_ctrl, b->h_ctrl, b->n * sizeof(Ctrl), cudaMemcpyHostToDevice) != cudaSuccess)
     return done(bcuda(failed_call_error(), "upload ensemble tables"));
   // CFL accumulators of every scenario from its initial state (with ghosts).
-  if (launch_cfl_batch(b->d_args1, b->d_tile_scn, 0, b->total_tiles, b->grid, b->stream))
+  if (b->ops->cfl_batch(b->d_args1, b->d_tile_scn, 0, b->total_tiles, b->grid, b->stream))
     return done(bcuda(failed_call_error(), "initial CFL"));
   if (cudaStreamSynchronize(b->stream) != cudaSuccess)
     return done(bcuda(failed_call_error(), "initial CFL"));

@@ -37,6 +37,11 @@
 
 using namespace hf;
 
+// A calibration handle runs every kernel (forward solve, tangent, adjoint)
+// on the 32 x 8 tiles of this build, with one tile numbering and one
+// forcing table for all of them.
+static_assert(TY == kGeomTileH[kGeomSmall], "calibration handles use the 32 x 8 geometry");
+
 namespace {
 
 int cfail(int code, const std::string& m) { return record_error(code, m.c_str()); }
@@ -281,7 +286,7 @@ int forward_run(hf_calib* c, int mode, bool checkpoints, int64_t* n_run) {
   const bool replay = mode == 1;
   const bool dual = mode == 2;
   C_TRY(init_ctrl(c, replay));
-  const ForcingDev fd = c->forcing.dev();
+  const ForcingDev fd = c->forcing.dev(kGeomSmall);
   StageArgs a1 = calib_args(c, c->U, c->U1, nullptr, 0, 0, c->ctrl, fd);
   const bool ssp = c->cfg.integrator == HF_SSPRK2;
   StageArgs a2 = calib_args(c, c->U1, c->U, c->U, ssp ? 1 : 0, 1, c->ctrl, fd);
@@ -393,7 +398,7 @@ int recompute_segment(hf_calib* c, int64_t j, int b) {
   const size_t bytes = (size_t)nb * sizeof(double);
   const bool ssp = c->cfg.integrator == HF_SSPRK2;
   double* buf = seg_buf(c, b);
-  const ForcingDev fd = c->forcing.dev();
+  const ForcingDev fd = c->forcing.dev(kGeomSmall);
   cudaStream_t st = c->s_rec;
   for (int f = 0; f < 3; ++f)
     C_CUDA(cudaMemcpyAsync(slot(buf, 0, f, nb), slot(c->ckpt, j, f, nb), bytes,
@@ -424,7 +429,7 @@ int reverse_segment(hf_calib* c, int64_t j, int b) {
   const int64_t nb = c->ncell, k0 = j * c->C, k1 = std::min(k0 + c->C, c->last_run);
   const bool ssp = c->cfg.integrator == HF_SSPRK2;
   double* buf = seg_buf(c, b);
-  ForcingDev fd = c->forcing.dev();
+  ForcingDev fd = c->forcing.dev(kGeomSmall);
   fd.src_dh = c->dh_rev;
   cudaStream_t st = c->s_rev;
   const int nr = (int)c->nr, nc = (int)c->nc;
@@ -598,7 +603,7 @@ int forward_run_lanes(hf_calib* c, int lanes, int64_t* n_run) {
   for (int f = 0; f < 3; ++f)
     C_CUDA(cudaMemcpyAsync(c->U[f], h0[f], bytes, cudaMemcpyDeviceToDevice, c->stream));
   C_TRY(init_ctrl(c, false));
-  const ForcingDev fd = c->forcing.dev();
+  const ForcingDev fd = c->forcing.dev(kGeomSmall);
   const bool ssp = c->cfg.integrator == HF_SSPRK2;
   const long long stride = (long long)c->ncell;
   // One wave: lanes x grid CTAs within the resident capacity (a second,
@@ -765,7 +770,7 @@ int hf_calib_create(const hf_scenario_desc* d, int64_t n_steps, int64_t n_gauges
       cudaMemset(c->dn, 0, bytes) != cudaSuccess)
     return bail(ccuda(cudaErrorUnknown, "upload"));
   if ((rc = forcing_set_rain(c->forcing, d->n_rain, d->rain_t, d->rain_rate))) return bail(rc);
-  if ((rc = forcing_set_sources(c->forcing, nr, nc, c->tiles_x, c->tiles_y, d->n_sources,
+  if ((rc = forcing_set_sources(c->forcing, nr, nc, d->n_sources,
                                 d->src_rows, d->src_cols, d->src_offsets, d->src_t, d->src_q)))
     return bail(rc);
   c->grid = stage_grid_size(c->ntiles, device);

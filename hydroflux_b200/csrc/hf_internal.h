@@ -11,30 +11,47 @@
 
 namespace hf {
 
-// Tile geometry of the fused stage kernel: a CTA advances a TX x TY block of
-// cells; its shared-memory halo is 4 cells (two-cell dry buffer of the
-// slope limiter + one neighbour slope + one neighbour alpha). 32 x 8 tiles
-// take 66 KB of shared memory, so three CTAs (24 warps) fit on an SM: on the
-// 4096^2 valley this is 16% faster than 32 x 16 tiles at two CTAs per SM,
-// although it recomputes more halo faces (2.8 vs 2.5 faces per cell).
-#ifndef HF_TILE_X
-#define HF_TILE_X 32
-#endif
-#ifndef HF_TILE_Y
+// Tile geometry of the fused stage kernels: a CTA advances a TX x TY block
+// of cells, one cell per thread; its shared-memory halo is 4 cells (two-cell
+// dry buffer of the slope limiter + one neighbour slope + one neighbour
+// alpha). Two geometries are built (hf_tiles.cu is compiled once for each;
+// its symbols sit in the geometry's inline namespace):
+// - 32 x 8 (g8, kGeomSmall): 256 threads, 71 KB of shared memory, three CTAs
+//   (24 warps) per SM. Many tiles per grid, so small grids still spread over
+//   every SM. The DualD tangent, the adjoint, the strip kernel and the
+//   calibration handle's runs use this geometry only.
+// - 32 x 32 (g32, kGeomLarge): 1024 threads, 211 KB of shared memory, one
+//   CTA (32 warps) per SM. The halo is a smaller share of the tile (2.32
+//   Audusse+HLLC faces and 2.36 limited-slope cells per cell against 2.83
+//   and 3.0) and an SM runs more warps; a stage launch on the 4096^2 valley
+//   takes 2.06 ms against 2.36 ms. Grids with at least kLargeTilesMin tiles
+//   of it take it (geom_for).
+// Both compute every cell with the same operations: results are identical.
+constexpr int TX = 32;
+constexpr int kGeomSmall = 0, kGeomLarge = 1;
+constexpr int kGeomTileH[2] = {8, 32};
+constexpr int kLargeTilesMin = 100;
+#ifndef HF_GEOM
+#define HF_GEOM g8
+#define HF_GEOM_INDEX 0
 #define HF_TILE_Y 8
-#endif
-#ifndef HF_THREADS
 #define HF_THREADS 256
-#endif
-#ifndef HF_MIN_BLOCKS
 #define HF_MIN_BLOCKS 3
 #endif
-constexpr int TX = HF_TILE_X;
+// The build of the 32 x 8 geometry also carries the kernels that exist in
+// one geometry only (strip, DualD, adjoint) and the host code.
+#define HF_GEOM_PRIMARY (HF_GEOM_INDEX == 0)
+#define HF_CAT2(a, b) a##b
+#define HF_CAT(a, b) HF_CAT2(a, b)
+#define HF_GEOM_OPS HF_CAT(geom_ops_, HF_GEOM)
+inline namespace HF_GEOM {
 constexpr int TY = HF_TILE_Y;
 constexpr int NTHREADS = HF_THREADS;
 constexpr int ROWS_PER_PASS = NTHREADS / TX;           // tile rows one pass of the CTA covers
 constexpr int CELLS_PER_THREAD = TX * TY / NTHREADS;   // cells a thread updates per tile
 static_assert(NTHREADS % TX == 0 && TY % ROWS_PER_PASS == 0, "tile / thread shape");
+static_assert(TY == kGeomTileH[HF_GEOM_INDEX], "geometry index and tile height");
+}  // namespace HF_GEOM
 
 // Strip geometry of the streaming stage kernel (hf_strip.cuh): a CTA walks
 // down a TX-wide column of blocks of STRIP_ROWS rows, carrying the halo rows
@@ -188,14 +205,11 @@ struct StageArgs {
   TanPtrs tan;   // DualD kernels only
 };
 
-// Launchers (hf_kernels.cu).
-int launch_stage(const StageArgs& a, int grid, void* stream);
-int launch_finalize(const StageArgs& a, int grid, void* stream);
+// Launchers of the step control and standalone kernels (hf_kernels.cu).
 int launch_control(Ctrl* ctrl, double dx, double dy, const ForcingDev& f, void* stream);
 // Records one gauge row when the step ran (init: unconditionally, the peak
 // starting from 0).
 int launch_gauges(const Ctrl* ctrl, const double* h, const GaugeDev& g, int init, void* stream);
-int launch_cfl(const StageArgs& a, int with_ghosts, int grid, void* stream);
 int launch_set_fixed(Ctrl* ctrl, double dt, void* stream);
 int launch_set_step(Ctrl* ctrl, double dt_cap, double cfl, double max_dt, int check_finite,
                     void* stream);
@@ -208,7 +222,6 @@ int launch_rain(int64_t ncell, double* h, double* hu, double* hv, double rate, d
 int launch_point_sources(int64_t nc, double* h, double* hu, double* hv, int n,
                          const int64_t* rows, const int64_t* cols, const double* q, double dt,
                          double dx, double dy, void* stream);
-// *count += cells with !(n >= 0) (count is device memory, zeroed by the caller).
 // max_depth_exceeds_relief reduction (sim.rs:248-271) into c->relief_keys,
 // which the caller presets to {0, 0, ~0}. Decode with relief_key_value.
 int launch_relief(int64_t ncell, const double* h, const double* z, Ctrl* c, void* stream);
@@ -218,18 +231,52 @@ inline double relief_key_value(unsigned long long k) {
   std::memcpy(&d, &b, sizeof d);
   return d;
 }
+// *count += cells with !(n >= 0) (count is device memory, zeroed by the caller).
 int launch_count_bad_manning(int64_t ncell, const double* n, unsigned long long* count,
                              void* stream);
 int launch_hllc(int x_dir, int64_t n, const double* ul, const double* ur, double* out,
                 void* stream);
-int stage_grid_size(int tiles, int device);
-size_t stage_smem_bytes();
 
 // TMA descriptors of one stage's inputs for the strip kernel (hf_strip.cuh):
 // depth rows (box 40 x (STRIP_ROWS + 1)), bed, hu, hv (40 x STRIP_ROWS).
 struct StripMaps {
   CUtensorMap h, z, hu, hv;
 };
+
+// The tile-shaped kernels of one geometry (hf_tiles.cu), reached from host
+// code that serves grids of either geometry through geom_ops().
+struct GeomOps {
+  int tile_h;   // TY of the geometry (the width is TX)
+  int threads;  // CTA size
+  // CTAs for `tiles` tiles on `device` (also raises the kernels' shared-memory
+  // limits; never inside a stream capture).
+  int (*grid_size)(int tiles, int device);
+  int (*stage)(const StageArgs& a, int grid, void* stream);
+  int (*finalize)(const StageArgs& a, int grid, void* stream);
+  int (*cfl)(const StageArgs& a, int with_ghosts, int grid, void* stream);
+  int (*stage_batch)(const StageArgs* args, const int* tile_scn, const int* n_tiles, int grid,
+                     void* stream, const int* tile_local, int* counter);
+  int (*cfl_batch)(const StageArgs* args, const int* tile_scn, int first_tile, int last_tile,
+                   int grid, void* stream);
+};
+const GeomOps& geom_ops_g8();
+const GeomOps& geom_ops_g32();
+const GeomOps& geom_ops(int geom);
+// The geometry of an nr x nc grid: kGeomLarge once it has kLargeTilesMin
+// tiles of 32 x 32, else kGeomSmall.
+int geom_for(int64_t nr, int64_t nc);
+inline int tiles_along(int64_t n, int tile) { return (int)((n + tile - 1) / tile); }
+
+inline namespace HF_GEOM {
+// The single-grid stage (k_stage_pf), the forward-Euler finalize and the CFL
+// reduction of this geometry. Callers size the grid with stage_grid_size()
+// first, which also raises the kernels' shared-memory limits on the device.
+int launch_stage(const StageArgs& a, int grid, void* stream);
+int launch_finalize(const StageArgs& a, int grid, void* stream);
+int launch_cfl(const StageArgs& a, int with_ghosts, int grid, void* stream);
+int stage_grid_size(int tiles, int device);
+size_t stage_smem_bytes();
+
 // Encodes the descriptors of a stage's inputs (a.in_h, a.z, a.in_hu,
 // a.in_hv); false when the grid cannot be fetched that way (an odd column
 // count gives rows that do not start on 16 bytes; an unaligned buffer; no
@@ -276,6 +323,7 @@ int launch_calib_rewind(Ctrl* c, const double* ts, long long k, void* stream);
 int launch_calib_ckpt(const Ctrl* c, const double* h, const double* hu, const double* hv,
                       double* ckpt, long long every, long long cap, long long ncell,
                       void* stream);
+}  // namespace HF_GEOM
 
 // Sets the calling thread's hf_last_error() message and returns `code`.
 int record_error(int code, const char* msg);
@@ -321,33 +369,40 @@ struct ForcingHost {
   int* d_off = nullptr;
   double* d_st = nullptr;
   double* d_sq = nullptr;
-  int* d_tile_start = nullptr;
-  int* d_tile_order = nullptr;
+  int* d_tile_start[2] = {nullptr, nullptr};  // per geometry (kGeomSmall, kGeomLarge)
+  int* d_tile_order[2] = {nullptr, nullptr};
   int* d_blk_start = nullptr;
   int* d_blk_order = nullptr;
   double* d_dh = nullptr;
   SeriesUnits rain_u, src_u;
   void release_rain();
   void release_src();
-  ForcingDev dev() const;
+  // The device tables, with the point sources bucketed by the tiles of
+  // geometry `geom`.
+  ForcingDev dev(int geom) const;
 };
 // Validate and upload a rain series / point-source series (see
-// hf_sim_set_rain / hf_sim_set_point_sources); sources are bucketed by tile.
+// hf_sim_set_rain / hf_sim_set_point_sources); sources are bucketed by the
+// tiles of both geometries and by strip block.
 int forcing_set_rain(ForcingHost& f, int64_t n_points, const double* t, const double* rate);
-int forcing_set_sources(ForcingHost& f, int64_t nr, int64_t nc, int tiles_x, int tiles_y,
-                        int64_t n_sources, const int64_t* rows, const int64_t* cols,
-                        const int64_t* offsets, const double* t, const double* q);
+int forcing_set_sources(ForcingHost& f, int64_t nr, int64_t nc, int64_t n_sources,
+                        const int64_t* rows, const int64_t* cols, const int64_t* offsets,
+                        const double* t, const double* q);
 
-// Ensemble launchers (hf_kernels.cu): args1/args2 are per-scenario device
-// arrays of stage-1 / stage-2 arguments, ctrls the per-scenario control blocks.
-// n_tiles is a device int (the tile list length, read at launch time); the
-// CFL reduction covers tiles [first_tile, last_tile).
-// tile_local / counter select the schedule (see k_stage_batch); the defaults
-// are the static stride over scenario-contiguous tiles.
+// Ensemble launchers: args1/args2 are per-scenario device arrays of stage-1 /
+// stage-2 arguments, ctrls the per-scenario control blocks. n_tiles is a
+// device int (the tile list length, read at launch time); the CFL reduction
+// covers tiles [first_tile, last_tile). tile_local / counter select the
+// schedule (see k_stage_batch): nullptr gives the static stride over
+// scenario-contiguous tiles. The stage and CFL launchers are per geometry
+// (hf_tiles.cu, GeomOps::stage_batch / cfl_batch); control and commit are
+// not (hf_kernels.cu).
+inline namespace HF_GEOM {
 int launch_stage_batch(const StageArgs* args, const int* tile_scn, const int* n_tiles, int grid,
-                       void* stream, const int* tile_local = nullptr, int* counter = nullptr);
+                       void* stream, const int* tile_local, int* counter);
 int launch_cfl_batch(const StageArgs* args, const int* tile_scn, int first_tile, int last_tile,
                      int grid, void* stream);
+}  // namespace HF_GEOM
 // counters (2 ints, may be NULL) are zeroed for the dynamic schedule.
 int launch_batch_control(Ctrl* ctrls, const StageArgs* args, int n, void* stream,
                          int* counters = nullptr);

@@ -130,12 +130,13 @@ extern "C" int hf_ssprk2_step_noalloc(const hf_grid* grid, double* h, double* hu
     cudaGetLastError();
     return noalloc_fail(HF_ERR_CUDA, std::string("cudaMemsetAsync: ") + cudaGetErrorString(e));
   }
+  const GeomOps& o = geom_ops(geom_for(grid->n_rows, grid->n_cols));
   StageArgs a;
   std::memset(&a, 0, sizeof a);
   a.nr = (int)grid->n_rows;
   a.nc = (int)grid->n_cols;
-  a.tiles_x = (int)((grid->n_cols + TX - 1) / TX);
-  a.tiles_y = (int)((grid->n_rows + TY - 1) / TY);
+  a.tiles_x = tiles_along(grid->n_cols, TX);
+  a.tiles_y = tiles_along(grid->n_rows, o.tile_h);
   a.dx = grid->dx;
   a.dy = grid->dy;
   a.rx = hfa::make_recip(a.dx);
@@ -144,18 +145,18 @@ extern "C" int hf_ssprk2_step_noalloc(const hf_grid* grid, double* h, double* hu
   a.n = grid->manning;
   a.bc = boundaries_dev(b);
   a.ctrl = ctrl;
-  const int gsz = stage_grid_size(a.tiles_x * a.tiles_y, device);
+  const int gsz = o.grid_size(a.tiles_x * a.tiles_y, device);
   if (launch_set_fixed(ctrl, dt, stream)) return launch_failed();
   // Stage 1: U -> scratch (every real cell of h1/hu1/hv1 is written before
   // stage 2 reads it, so the stale stage buffer needs no clearing).
   a.in_h = h; a.in_hu = hu; a.in_hv = hv;
   a.out_h = h1; a.out_hu = hu1; a.out_hv = hv1;
   a.un_h = h; a.un_hu = hu; a.un_hv = hv;
-  if (launch_stage(a, gsz, stream)) return launch_failed();
+  if (o.stage(a, gsz, stream)) return launch_failed();
   // Stage 2 + convex combination, in place on the caller's state.
   a.in_h = h1; a.in_hu = hu1; a.in_hv = hv1;
   a.out_h = h; a.out_hu = hu; a.out_hv = hv;
   a.combine = 1;
-  if (launch_stage(a, gsz, stream)) return launch_failed();
+  if (o.stage(a, gsz, stream)) return launch_failed();
   return HF_OK;
 }

@@ -75,6 +75,10 @@ struct Slot {
 struct hf_server {
   int device = 0;
   cudaStream_t stream = nullptr;
+  // The server's batched kernels run on 32 x 32 tiles: a served mix is
+  // dominated by the grids large enough to fill the GPU.
+  int geom = kGeomLarge;
+  const GeomOps* ops = nullptr;
   uint64_t budget = 0, in_use = 0;
   int max_slots = 0;
   int grid = 1;
@@ -150,9 +154,9 @@ int rebuild_tiles(hf_server* v) {
 // server changes all the time.
 int enqueue_serve_step(hf_server* v) {
   if (launch_batch_control(v->d_ctrl, v->d_args1, v->max_slots, v->stream, v->d_counters) ||
-      launch_stage_batch(v->d_args1, v->d_tile_scn, v->d_n_tiles, v->grid, v->stream, nullptr,
+      v->ops->stage_batch(v->d_args1, v->d_tile_scn, v->d_n_tiles, v->grid, v->stream, nullptr,
                          v->d_counters) ||
-      launch_stage_batch(v->d_args2, v->d_tile_scn, v->d_n_tiles, v->grid, v->stream, nullptr,
+      v->ops->stage_batch(v->d_args2, v->d_tile_scn, v->d_n_tiles, v->grid, v->stream, nullptr,
                          v->d_counters + 1) ||
       launch_batch_commit(v->d_ctrl, v->max_slots, v->stream))
     return scuda(failed_call_error(), "enqueue serve step");
@@ -212,12 +216,14 @@ int hf_server_create(int device, uint64_t hbm_budget_bytes, int max_slots, hf_se
   v->budget = hbm_budget_bytes;
   v->max_slots = max_slots;
   v->slots.resize(max_slots);
-  // Every tile holds at most TX*TY cells of 64 B; partial edge tiles add at
-  // most (rows/TY + cols/TX + 1) per scenario, bounded here generously.
-  const uint64_t full_tiles = hbm_budget_bytes / (64ull * TX * TY);
+  v->ops = &geom_ops(v->geom);
+  // Every tile holds at most TX * tile_h cells of 64 B; partial edge tiles
+  // add at most (rows / tile_h + cols / TX + 1) per scenario, bounded here
+  // generously.
+  const uint64_t full_tiles = hbm_budget_bytes / (64ull * TX * v->ops->tile_h);
   const uint64_t cap = full_tiles + 4096ull * (uint64_t)max_slots;
   v->tile_cap = (int)std::min<uint64_t>(cap, (uint64_t)INT_MAX / 2);
-  v->grid = stage_grid_size(std::max(v->tile_cap, 1), device);
+  v->grid = v->ops->grid_size(std::max(v->tile_cap, 1), device);
   if (cudaStreamCreateWithFlags(&v->stream, cudaStreamNonBlocking) != cudaSuccess)
     return done(scuda(failed_call_error(), "cudaStreamCreate"));
   if (cudaMalloc((void**)&v->d_ctrl, max_slots * sizeof(Ctrl)) != cudaSuccess ||
@@ -279,8 +285,8 @@ int hf_server_admit(hf_server* v, const hf_scenario_desc* d, int* slot_out) {
   s.nc = nc;
   s.bytes = bytes;
   s.t_end = d->t_end;
-  s.tiles_x = (int)((nc + TX - 1) / TX);
-  s.tiles_y = (int)((nr + TY - 1) / TY);
+  s.tiles_x = tiles_along(nc, TX);
+  s.tiles_y = tiles_along(nr, v->ops->tile_h);
   auto undo = [&](int code) {
     free_slot(s);
     return code;
@@ -304,7 +310,7 @@ int hf_server_admit(hf_server* v, const hf_scenario_desc* d, int* slot_out) {
   }
   int rc = forcing_set_rain(s.forcing, d->n_rain, d->rain_t, d->rain_rate);
   if (rc == HF_OK)
-    rc = forcing_set_sources(s.forcing, nr, nc, s.tiles_x, s.tiles_y, d->n_sources, d->src_rows,
+    rc = forcing_set_sources(s.forcing, nr, nc, d->n_sources, d->src_rows,
                              d->src_cols, d->src_offsets, d->src_t, d->src_q);
   if (rc != HF_OK) return undo(rc);
   StageArgs& x = s.a1;
@@ -322,7 +328,7 @@ int hf_server_admit(hf_server* v, const hf_scenario_desc* d, int* slot_out) {
   x.bc = boundaries_dev(d->cfg.boundaries);
   x.ctrl = v->d_ctrl + k;
   x.dry_tol = d->cfg.friction_dry_tol;
-  x.f = s.forcing.dev();
+  x.f = s.forcing.dev(v->geom);
   StageArgs y = x;
   x.in_h = h; x.in_hu = hu; x.in_hv = hv;
   x.out_h = h1; x.out_hu = hu1; x.out_hv = hv1;
@@ -352,7 +358,7 @@ int hf_server_admit(hf_server* v, const hf_scenario_desc* d, int* slot_out) {
   }
   // CFL accumulators of the new scenario from its initial state.
   const int tb = s.a1.tile_base;
-  if (launch_cfl_batch(v->d_args1, v->d_tile_scn, tb, tb + s.tiles_x * s.tiles_y, v->grid,
+  if (v->ops->cfl_batch(v->d_args1, v->d_tile_scn, tb, tb + s.tiles_x * s.tiles_y, v->grid,
                        v->stream) ||
       cudaStreamSynchronize(v->stream) != cudaSuccess)
     return scuda(failed_call_error(), "initial CFL");

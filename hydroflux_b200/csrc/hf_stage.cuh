@@ -15,6 +15,7 @@
 #include "hf_internal.h"
 
 namespace hf {
+inline namespace HF_GEOM {
 
 namespace {
 
@@ -978,4 +979,5 @@ __device__ __forceinline__ bool interior_tile(const StageArgs& A, int tile) {
   return gi0 >= 4 && gj0 >= 4 && gi0 + TY + 4 <= A.nr && gj0 + TX + 4 <= A.nc;
 }
 
+}  // namespace HF_GEOM
 }  // namespace hf

@@ -34,6 +34,7 @@
 #include "hf_stage.cuh"
 
 namespace hf {
+inline namespace HF_GEOM {
 
 namespace {
 
@@ -339,4 +340,5 @@ __device__ __forceinline__ void strip_update(const StageArgs& A, StripSmem& S, i
 
 }  // namespace
 
+}  // namespace HF_GEOM
 }  // namespace hf

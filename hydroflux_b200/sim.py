@@ -345,11 +345,13 @@ class Simulation:
         raise_for(lib().hf_sim_get_state(self._h, h.ctypes.data, hu.ctypes.data, hv.ctypes.data))
         return h, hu, hv
 
-    STAGE_KERNELS = {"auto": 0, "tile": 1, "strip": 2}
+    STAGE_KERNELS = {"auto": 0, "tile": 1, "strip": 2, "tile32": 3}
 
     def set_stage_kernel(self, kind: str) -> None:
-        """'tile', 'strip' or 'auto' (hf_sim_set_stage_kernel): which kernel
-        runs the stages; results are bit-identical."""
+        """'tile' (32 x 8 tiles), 'tile32' (32 x 32 tiles), 'strip' or 'auto'
+        (hf_sim_set_stage_kernel): which kernel runs the stages; auto takes
+        tile32 on grids of at least 100 tiles of 32 x 32, else tile. Results
+        are bit-identical."""
         raise_for(lib().hf_sim_set_stage_kernel(self._h, self.STAGE_KERNELS[kind]))
 
     def stage_kernel(self) -> str:

@@ -165,15 +165,19 @@ int hf_sim_set_state_aos(hf_sim* sim, const double* hhuhv);
 /* Simulation::set_boundaries (sim.rs:194-196). */
 int hf_sim_set_boundaries(hf_sim* sim, const hf_boundaries* bcs);
 /* Which kernel runs the stages of a simulation; no counterpart in the
- * reference (its passes are fixed). HF_STAGE_TILE recomputes every 32 x 8
- * tile with its halo; HF_STAGE_STRIP walks 32-column strips in 7-row blocks
- * and carries the halo rows from block to block (fewer faces and slopes per
- * cell, TMA row fetches; needs an even column count). HF_STAGE_AUTO (the
- * default at creation) takes the tile kernel, which measured faster on B200.
+ * reference (its passes are fixed). HF_STAGE_TILE computes every 32 x 8
+ * tile with its halo (three 256-thread CTAs per SM); HF_STAGE_TILE32 every
+ * 32 x 32 tile (one 1024-thread CTA per SM: a smaller halo share, more warps
+ * per SM; faster once a grid has enough tiles to fill the GPU);
+ * HF_STAGE_STRIP walks 32-column strips in 7-row blocks and carries the halo
+ * rows from block to block (fewer faces and slopes per cell, TMA row
+ * fetches; needs an even column count). HF_STAGE_AUTO (the default at
+ * creation) takes HF_STAGE_TILE32 for grids of at least 100 tiles of 32 x 32
+ * and HF_STAGE_TILE below; hf_sim_stage_kernel reports the kernel in use.
  * Results are bit-identical; this is a tuning and diagnostic knob. Forcing
- * HF_STAGE_STRIP where it cannot run returns HF_ERR_UNSUPPORTED (the tile
- * kernel stays selected). */
-enum { HF_STAGE_AUTO = 0, HF_STAGE_TILE = 1, HF_STAGE_STRIP = 2 };
+ * HF_STAGE_STRIP where it cannot run returns HF_ERR_UNSUPPORTED (the auto
+ * choice stays selected). */
+enum { HF_STAGE_AUTO = 0, HF_STAGE_TILE = 1, HF_STAGE_STRIP = 2, HF_STAGE_TILE32 = 3 };
 int hf_sim_set_stage_kernel(hf_sim* sim, int kind);
 int hf_sim_stage_kernel(const hf_sim* sim, int* kind);
 /* The state fields of simulation handles come from a per-device memory pool

@@ -40,6 +40,7 @@ pub const HF_SSPRK2: i32 = 1;
 pub const HF_STAGE_AUTO: c_int = 0;
 pub const HF_STAGE_TILE: c_int = 1;
 pub const HF_STAGE_STRIP: c_int = 2;
+pub const HF_STAGE_TILE32: c_int = 3;
 pub const HF_NOALLOC_MAX_CELLS: i64 = 1 << 20;
 
 #[repr(C)] #[derive(Clone, Copy)]

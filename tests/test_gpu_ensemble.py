@@ -124,3 +124,28 @@ def test_autotuner_picks_a_schedule_and_changes_nothing(gpu):
             assert exact_fraction(ens.states(k), ref) == 1.0, f"scenario {k}"
         with pytest.raises(ValueError):
             ens.set_schedule(4)
+
+
+@pytest.mark.parametrize("schedule", [0, 1])
+def test_ensemble_on_32x32_tiles(gpu, schedule):
+    """With a 352 x 352 scenario beside the small ones the ensemble has at
+    least 100 tiles of 32 x 32 and runs its batched kernels on that geometry
+    (the lone solves of the small scenarios run on 32 x 8 tiles): every
+    scenario still equals its lone solve bit for bit, after the same steps."""
+    ensemble, workloads = gpu
+    scns = mixed_scenarios(workloads)
+    big = workloads.valley(n=352, dx=5.0, seed=77, t_end=1e9)
+    big.max_dt = 5.0
+    scns.append(big)
+    tiles32 = sum(-(-s.shape[0] // 32) * -(-s.shape[1] // 32) for s in scns)
+    assert tiles32 >= 100
+    with ensemble.Ensemble(scns) as ens:
+        ens.set_schedule(schedule)
+        ens.run(max_batch_steps=30)
+        for k, s in enumerate(scns):
+            info = ens.info(k)
+            assert info["status"] == 0 and info["steps"] > 0
+            with workloads.simulation_for(s) as sim:
+                sim.run_steps(info["steps"], s.t_end)
+                assert sim.steps() == info["steps"] and sim.time() == info["t"]
+                assert exact_fraction(ens.states(k), sim.states()) == 1.0, f"scenario {k}"

@@ -98,15 +98,18 @@ def test_strip_forcing_against_oracle(gpu, oracle, integrator):
 
 
 def test_strip_selection(gpu):
-    """The default is the tile kernel; the strip kernel is taken when asked
-    for, on any grid with an even column count."""
+    """The default is a tile kernel (32 x 32 tiles on a large grid, 32 x 8 on
+    a small one); the strip kernel is taken when asked for, on any grid with
+    an even column count."""
     sim = gpu
     zero = np.zeros((2048, 2048))
     with sim.Simulation(sim.Mesh2D(zero, 1.0, 1.0, 0.03), (zero + 1.0, zero, zero),
                         sim.SimulationConfig()) as s:
-        assert s.stage_kernel() == "tile"
+        assert s.stage_kernel() == "tile32"
         s.set_stage_kernel("strip")
         assert s.stage_kernel() == "strip"
+        s.set_stage_kernel("auto")
+        assert s.stage_kernel() == "tile32"
     small = np.zeros((64, 64))
     with sim.Simulation(sim.Mesh2D(small, 1.0, 1.0, 0.03), (small + 1.0, small, small),
                         sim.SimulationConfig()) as s:
