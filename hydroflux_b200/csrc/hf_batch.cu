@@ -72,11 +72,16 @@ constexpr int kSchedules = 4;  // bit 0: dynamic; bit 1: largest scenarios first
 struct hf_batch {
   int device = 0;
   cudaStream_t stream = nullptr;
-  // Tile geometry of the batched kernels: 32 x 32 once the ensemble has
-  // kLargeTilesMin such tiles (the tiles of all scenarios fill the GPU),
-  // else 32 x 8.
+  // Tile geometry of the batched kernels: 32 x 32 once the batched scenarios
+  // have kLargeTilesMin such tiles between them, else 32 x 8.
   int geom = kGeomSmall;
   const GeomOps* ops = nullptr;
+  // Scenarios of at least kSoloTilesMin tiles of 32 x 32 are not in the tile
+  // lists: each stage runs them as their own k_stage_pf launches on 32 x 32
+  // tiles, with these arguments (batched = 1) and grids.
+  std::vector<int> solo;
+  std::vector<StageArgs> solo_a1, solo_a2;
+  std::vector<int> solo_grid;
   int n = 0;
   int64_t total_cells = 0;
   int total_tiles = 0;
@@ -138,10 +143,17 @@ int enqueue_batch_step(hf_batch* b, int sched) {
   int* c2 = dynamic ? b->d_counters + 1 : nullptr;
   if (launch_batch_control(b->d_ctrl, b->d_args1, b->n, b->stream, dynamic ? b->d_counters : nullptr))
     return bcuda(failed_call_error(), "control");
+  const GeomOps& large = geom_ops(kGeomLarge);
   if (b->ops->stage_batch(b->d_args1, scn, b->d_n_tiles, b->grid, b->stream, local, c1))
     return bcuda(failed_call_error(), "stage 1");
+  for (size_t k = 0; k < b->solo.size(); ++k)
+    if (large.stage(b->solo_a1[k], b->solo_grid[k], b->stream))
+      return bcuda(failed_call_error(), "stage 1");
   if (b->ops->stage_batch(b->d_args2, scn, b->d_n_tiles, b->grid, b->stream, local, c2))
     return bcuda(failed_call_error(), "stage 2");
+  for (size_t k = 0; k < b->solo.size(); ++k)
+    if (large.stage(b->solo_a2[k], b->solo_grid[k], b->stream))
+      return bcuda(failed_call_error(), "stage 2");
   if (launch_batch_commit(b->d_ctrl, b->n, b->stream)) return bcuda(failed_call_error(), "commit");
   return HF_OK;
 }
@@ -267,8 +279,10 @@ int hf_batch_create(int64_t n_scenarios, const hf_scenario_desc* sc, int device,
     }
     total += nc;
     const int64_t tx = tiles_along(d.mesh.n_cols, TX);
+    const int64_t t32 = tx * tiles_along(d.mesh.n_rows, kGeomTileH[kGeomLarge]);
+    if (t32 >= kSoloTilesMin) continue;  // runs its own launches
     tiles += tx * tiles_along(d.mesh.n_rows, kGeomTileH[kGeomSmall]);
-    tiles_large += tx * tiles_along(d.mesh.n_rows, kGeomTileH[kGeomLarge]);
+    tiles_large += t32;
   }
   const int geom = tiles_large >= kLargeTilesMin ? kGeomLarge : kGeomSmall;
   if (geom == kGeomLarge) tiles = tiles_large;
@@ -290,7 +304,7 @@ int hf_batch_create(int64_t n_scenarios, const hf_scenario_desc* sc, int device,
   b->total_tiles = (int)tiles;
   b->geom = geom;
   b->ops = &geom_ops(geom);
-  b->grid = b->ops->grid_size(b->total_tiles, device);
+  b->grid = b->ops->grid_size(std::max(b->total_tiles, 1), device);
   b->forcing.resize(b->n);
   if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
     return done(bcuda(failed_call_error(), "cudaStreamCreate"));
@@ -299,13 +313,14 @@ int hf_batch_create(int64_t n_scenarios, const hf_scenario_desc* sc, int device,
   double* f = b->buf;
   b->h = f; b->hu = f + total; b->hv = f + 2 * total; b->h1 = f + 3 * total;
   b->hu1 = f + 4 * total; b->hv1 = f + 5 * total; b->z = f + 6 * total; b->nman = f + 7 * total;
+  const size_t list_len = (size_t)std::max(b->total_tiles, 1);  // solo scenarios only: empty lists
   if (cudaMalloc((void**)&b->d_ctrl, b->n * sizeof(Ctrl)) != cudaSuccess ||
       cudaMalloc((void**)&b->d_args1, b->n * sizeof(StageArgs)) != cudaSuccess ||
       cudaMalloc((void**)&b->d_args2, b->n * sizeof(StageArgs)) != cudaSuccess ||
-      cudaMalloc((void**)&b->d_tile_scn, b->total_tiles * sizeof(int)) != cudaSuccess ||
-      cudaMalloc((void**)&b->d_tile_scn_lpt, b->total_tiles * sizeof(int)) != cudaSuccess ||
-      cudaMalloc((void**)&b->d_tile_local, b->total_tiles * sizeof(int)) != cudaSuccess ||
-      cudaMalloc((void**)&b->d_tile_local_lpt, b->total_tiles * sizeof(int)) != cudaSuccess ||
+      cudaMalloc((void**)&b->d_tile_scn, list_len * sizeof(int)) != cudaSuccess ||
+      cudaMalloc((void**)&b->d_tile_scn_lpt, list_len * sizeof(int)) != cudaSuccess ||
+      cudaMalloc((void**)&b->d_tile_local, list_len * sizeof(int)) != cudaSuccess ||
+      cudaMalloc((void**)&b->d_tile_local_lpt, list_len * sizeof(int)) != cudaSuccess ||
       cudaMalloc((void**)&b->d_counters, 2 * sizeof(int)) != cudaSuccess ||
       cudaMalloc((void**)&b->d_n_tiles, sizeof(int)) != cudaSuccess ||
       cudaMallocHost((void**)&b->h_ctrl, b->n * sizeof(Ctrl)) != cudaSuccess)
@@ -336,7 +351,10 @@ int hf_batch_create(int64_t n_scenarios, const hf_scenario_desc* sc, int device,
       if (cudaMemcpy(b->nman + o, nn.data(), bytes, cudaMemcpyHostToDevice) != cudaSuccess)
         return done(bcuda(failed_call_error(), "upload manning"));
     }
-    const int tx = tiles_along(nc, TX), ty = tiles_along(nr, b->ops->tile_h);
+    const bool solo = (int64_t)tiles_along(nc, TX) * tiles_along(nr, kGeomTileH[kGeomLarge]) >=
+                      kSoloTilesMin;
+    const GeomOps& go = solo ? geom_ops(kGeomLarge) : *b->ops;
+    const int tx = tiles_along(nc, TX), ty = tiles_along(nr, go.tile_h);
     int rc = forcing_set_rain(b->forcing[s], d.n_rain, d.rain_t, d.rain_rate);
     if (rc == HF_OK)
       rc = forcing_set_sources(b->forcing[s], nr, nc, d.n_sources, d.src_rows, d.src_cols,
@@ -355,7 +373,8 @@ int hf_batch_create(int64_t n_scenarios, const hf_scenario_desc* sc, int device,
     x.nc = (int)nc;
     x.tiles_x = tx;
     x.tiles_y = ty;
-    x.tile_base = tb;
+    x.tile_base = solo ? 0 : tb;
+    x.batched = 1;
     x.dx = d.mesh.dx;
     x.dy = d.mesh.dy;
     x.rx = hfa::make_recip(x.dx);
@@ -365,7 +384,7 @@ int hf_batch_create(int64_t n_scenarios, const hf_scenario_desc* sc, int device,
     x.bc = boundaries_dev(d.cfg.boundaries);
     x.ctrl = b->d_ctrl + s;
     x.dry_tol = d.cfg.friction_dry_tol;
-    x.f = b->forcing[s].dev(b->geom);
+    x.f = b->forcing[s].dev(solo ? kGeomLarge : b->geom);
     StageArgs y = x;
     x.in_h = b->h + o; x.in_hu = b->hu + o; x.in_hv = b->hv + o;
     x.out_h = b->h1 + o; x.out_hu = b->hu1 + o; x.out_hv = b->hv1 + o;
@@ -376,34 +395,42 @@ int hf_batch_create(int64_t n_scenarios, const hf_scenario_desc* sc, int device,
     y.combine = 1;
     y.finalize = 1;
     a2[s] = y;
+    o += ncell;
+    if (solo) {
+      b->solo.push_back(s);
+      b->solo_a1.push_back(x);
+      b->solo_a2.push_back(y);
+      b->solo_grid.push_back(go.grid_size(tx * ty, device));
+      b->tiles_of.push_back(0);
+      continue;
+    }
     for (int t = 0; t < tx * ty; ++t) {
       tile_scn[tb + t] = s;
       tile_local[tb + t] = t;
     }
     b->tiles_of.push_back(tx * ty);
     tb += tx * ty;
-    o += ncell;
   }
   b->listed = b->n;
   // Order 1: the same tiles, scenarios by decreasing tile count (stable).
   std::vector<int> by_size(b->n), tile_scn_lpt, tile_local_lpt;
   for (int s = 0; s < b->n; ++s) by_size[s] = s;
-  std::stable_sort(by_size.begin(), by_size.end(), [&](int x, int y) {
-    return a1[x].tiles_x * a1[x].tiles_y > a1[y].tiles_x * a1[y].tiles_y;
-  });
+  std::stable_sort(by_size.begin(), by_size.end(),
+                   [&](int x, int y) { return b->tiles_of[x] > b->tiles_of[y]; });
   tile_scn_lpt.reserve(b->total_tiles);
   tile_local_lpt.reserve(b->total_tiles);
   for (int s : by_size)
-    for (int t = 0; t < a1[s].tiles_x * a1[s].tiles_y; ++t) {
+    for (int t = 0; t < b->tiles_of[s]; ++t) {
       tile_scn_lpt.push_back(s);
       tile_local_lpt.push_back(t);
     }
   if (cudaMemcpy(b->d_args1, a1.data(), b->n * sizeof(StageArgs), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(b->d_args2, a2.data(), b->n * sizeof(StageArgs), cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemcpy(b->d_tile_scn, tile_scn.data(), b->total_tiles * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemcpy(b->d_tile_local, tile_local.data(), b->total_tiles * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemcpy(b->d_tile_scn_lpt, tile_scn_lpt.data(), b->total_tiles * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemcpy(b->d_tile_local_lpt, tile_local_lpt.data(), b->total_tiles * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
+      (b->total_tiles > 0 &&
+       (cudaMemcpy(b->d_tile_scn, tile_scn.data(), b->total_tiles * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(b->d_tile_local, tile_local.data(), b->total_tiles * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(b->d_tile_scn_lpt, tile_scn_lpt.data(), b->total_tiles * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(b->d_tile_local_lpt, tile_local_lpt.data(), b->total_tiles * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)) ||
       cudaMemset(b->d_counters, 0, 2 * sizeof(int)) != cudaSuccess ||
       cudaMemcpy(b->d_n_tiles, &b->total_tiles, sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(b->d_ctrl, b->h_ctrl, b->n * sizeof(Ctrl), cudaMemcpyHostToDevice) != cudaSuccess)
@@ -411,6 +438,9 @@ int hf_batch_create(int64_t n_scenarios, const hf_scenario_desc* sc, int device,
   // CFL accumulators of every scenario from its initial state (with ghosts).
   if (b->ops->cfl_batch(b->d_args1, b->d_tile_scn, 0, b->total_tiles, b->grid, b->stream))
     return done(bcuda(failed_call_error(), "initial CFL"));
+  for (size_t k = 0; k < b->solo.size(); ++k)
+    if (geom_ops(kGeomLarge).cfl(b->solo_a1[k], 1, b->solo_grid[k], b->stream))
+      return done(bcuda(failed_call_error(), "initial CFL"));
   if (cudaStreamSynchronize(b->stream) != cudaSuccess)
     return done(bcuda(failed_call_error(), "initial CFL"));
   *out = b;

@@ -155,7 +155,7 @@ StageArgs calib_args(const hf_calib* c, double* const in[3], double* const out[3
   a.tiles_x = c->tiles_x;
   a.tiles_y = c->tiles_y;
   a.tile_base = 0;
-  a.pad_ = 0;
+  a.batched = 0;
   a.dx = c->dx;
   a.dy = c->dy;
   a.rx = hfa::make_recip(a.dx);

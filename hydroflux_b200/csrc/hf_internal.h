@@ -31,6 +31,11 @@ constexpr int TX = 32;
 constexpr int kGeomSmall = 0, kGeomLarge = 1;
 constexpr int kGeomTileH[2] = {8, 32};
 constexpr int kLargeTilesMin = 100;
+// A scenario of an ensemble or server with at least this many 32 x 32 tiles
+// (about 3.5 waves of the 148 SMs; from 724 x 724 cells on) fills the GPU
+// by itself: it runs its stages as its own k_stage_pf launches (arguments
+// as kernel parameters) beside the batched launch of the other scenarios.
+constexpr int kSoloTilesMin = 512;
 #ifndef HF_GEOM
 #define HF_GEOM g8
 #define HF_GEOM_INDEX 0
@@ -180,7 +185,9 @@ struct StageArgs {
   int nr, nc;
   int tiles_x, tiles_y;
   int tile_base;  // first tile of this grid in an ensemble's tile list (0 alone)
-  int pad_;
+  // 1 for a grid of an ensemble or server that runs k_stage_pf on its own:
+  // its clock is committed by k_batch_commit, not by the stage kernel.
+  int batched = 0;
   double dx, dy;
   // 1/dx and 1/dy for the divisions by the spacing (hfa::div_recip); a
   // default (ok = false) falls back to the IEEE division.

@@ -68,6 +68,10 @@ struct Slot {
   double* buf = nullptr;  // h, hu, hv, h1, hu1, hv1, z, n
   ForcingHost forcing;
   StageArgs a1, a2;
+  // At least kSoloTilesMin tiles: the stages run as the slot's own
+  // k_stage_pf launches (grid solo_grid) instead of through the tile list.
+  bool solo = false;
+  int solo_grid = 0;
 };
 
 }  // namespace
@@ -93,6 +97,9 @@ struct hf_server {
   int* d_n_tiles = nullptr;
   int* d_counters = nullptr;  // dynamic tile schedule: stage 1 / stage 2 counters
   cudaGraphExec_t graphs[3] = {nullptr, nullptr, nullptr};
+  // Running solo slots; the graphs launch their stages, so they are rebuilt
+  // when this set changes.
+  std::vector<int> solo_set;
 };
 
 namespace {
@@ -124,7 +131,7 @@ void destroy_server(hf_server* v) {
 // Rebuild the tile list from the admitted, unfinished slots and upload the
 // tables (no work in flight: called between graph chunks).
 int rebuild_tiles(hf_server* v) {
-  std::vector<int> scn;
+  std::vector<int> scn, solo;
   scn.reserve(v->n_tiles + 1024);
   std::vector<StageArgs> a1(v->max_slots), a2(v->max_slots);
   for (int k = 0; k < v->max_slots; ++k) {
@@ -133,11 +140,23 @@ int rebuild_tiles(hf_server* v) {
     std::memset(&a2[k], 0, sizeof(StageArgs));
     a1[k].ctrl = a2[k].ctrl = v->d_ctrl + k;
     if (!s.used) continue;
-    s.a1.tile_base = s.a2.tile_base = (int)scn.size();
-    if (!s.finished)
-      for (int t = 0; t < s.tiles_x * s.tiles_y; ++t) scn.push_back(k);
+    s.a1.tile_base = s.a2.tile_base = s.solo ? 0 : (int)scn.size();
+    if (!s.finished) {
+      if (s.solo)
+        solo.push_back(k);
+      else
+        for (int t = 0; t < s.tiles_x * s.tiles_y; ++t) scn.push_back(k);
+    }
     a1[k] = s.a1;
     a2[k] = s.a2;
+  }
+  if (solo != v->solo_set) {  // the graphs launch the solo slots' stages: capture them again
+    S_CUDA(cudaStreamSynchronize(v->stream));
+    for (auto& ge : v->graphs) {
+      if (ge) graph_destroy(ge);
+      ge = nullptr;
+    }
+    v->solo_set = solo;
   }
   if ((int)scn.size() > v->tile_cap) return sfail(HF_ERR_CAPACITY, "tile list capacity exceeded");
   v->n_tiles = (int)scn.size();
@@ -155,10 +174,18 @@ int rebuild_tiles(hf_server* v) {
 int enqueue_serve_step(hf_server* v) {
   if (launch_batch_control(v->d_ctrl, v->d_args1, v->max_slots, v->stream, v->d_counters) ||
       v->ops->stage_batch(v->d_args1, v->d_tile_scn, v->d_n_tiles, v->grid, v->stream, nullptr,
-                         v->d_counters) ||
-      v->ops->stage_batch(v->d_args2, v->d_tile_scn, v->d_n_tiles, v->grid, v->stream, nullptr,
-                         v->d_counters + 1) ||
-      launch_batch_commit(v->d_ctrl, v->max_slots, v->stream))
+                          v->d_counters))
+    return scuda(failed_call_error(), "enqueue serve step");
+  for (int k : v->solo_set)
+    if (v->ops->stage(v->slots[k].a1, v->slots[k].solo_grid, v->stream))
+      return scuda(failed_call_error(), "enqueue serve step");
+  if (v->ops->stage_batch(v->d_args2, v->d_tile_scn, v->d_n_tiles, v->grid, v->stream, nullptr,
+                          v->d_counters + 1))
+    return scuda(failed_call_error(), "enqueue serve step");
+  for (int k : v->solo_set)
+    if (v->ops->stage(v->slots[k].a2, v->slots[k].solo_grid, v->stream))
+      return scuda(failed_call_error(), "enqueue serve step");
+  if (launch_batch_commit(v->d_ctrl, v->max_slots, v->stream))
     return scuda(failed_call_error(), "enqueue serve step");
   return HF_OK;
 }
@@ -287,6 +314,8 @@ int hf_server_admit(hf_server* v, const hf_scenario_desc* d, int* slot_out) {
   s.t_end = d->t_end;
   s.tiles_x = tiles_along(nc, TX);
   s.tiles_y = tiles_along(nr, v->ops->tile_h);
+  s.solo = (int64_t)s.tiles_x * s.tiles_y >= kSoloTilesMin;
+  s.solo_grid = s.solo ? v->ops->grid_size(s.tiles_x * s.tiles_y, v->device) : 0;
   auto undo = [&](int code) {
     free_slot(s);
     return code;
@@ -327,6 +356,7 @@ int hf_server_admit(hf_server* v, const hf_scenario_desc* d, int* slot_out) {
   x.n = nm;
   x.bc = boundaries_dev(d->cfg.boundaries);
   x.ctrl = v->d_ctrl + k;
+  x.batched = 1;
   x.dry_tol = d->cfg.friction_dry_tol;
   x.f = s.forcing.dev(v->geom);
   StageArgs y = x;
@@ -358,8 +388,9 @@ int hf_server_admit(hf_server* v, const hf_scenario_desc* d, int* slot_out) {
   }
   // CFL accumulators of the new scenario from its initial state.
   const int tb = s.a1.tile_base;
-  if (v->ops->cfl_batch(v->d_args1, v->d_tile_scn, tb, tb + s.tiles_x * s.tiles_y, v->grid,
-                       v->stream) ||
+  if ((s.solo ? v->ops->cfl(s.a1, 1, s.solo_grid, v->stream)
+              : v->ops->cfl_batch(v->d_args1, v->d_tile_scn, tb, tb + s.tiles_x * s.tiles_y,
+                                  v->grid, v->stream)) ||
       cudaStreamSynchronize(v->stream) != cudaSuccess)
     return scuda(failed_call_error(), "initial CFL");
   v->in_use += bytes;

@@ -131,7 +131,7 @@ __global__ void __launch_bounds__(NTHREADS, HF_MIN_BLOCKS) k_stage_pf(const Stag
   }
   if (A.finalize) {
     block_reduce_speeds(sxm, sym, nonfin, A.ctrl);
-    if (blockIdx.x == 0 && threadIdx.x == 0) commit_clock(A.ctrl);
+    if (blockIdx.x == 0 && threadIdx.x == 0 && !A.batched) commit_clock(A.ctrl);
   }
 }
 

@@ -149,3 +149,29 @@ def test_ensemble_on_32x32_tiles(gpu, schedule):
                 sim.run_steps(info["steps"], s.t_end)
                 assert sim.steps() == info["steps"] and sim.time() == info["t"]
                 assert exact_fraction(ens.states(k), sim.states()) == 1.0, f"scenario {k}"
+
+
+@pytest.mark.parametrize("with_small", [True, False])
+def test_ensemble_solo_scenarios(gpu, with_small):
+    """Scenarios of at least 512 tiles of 32 x 32 (here 736 x 736 and
+    768 x 768) leave the tile lists and run their stages as their own
+    k_stage_pf launches; with no small scenario the lists are empty. Every
+    scenario equals its lone solve bit for bit, over the same steps and to
+    the horizon."""
+    ensemble, workloads = gpu
+    big = []
+    for k, (n, t_end) in enumerate(((736, 20.0), (768, 1e9))):
+        s = workloads.valley(n=n, dx=5.0, seed=90 + k, peak=200.0, t_end=t_end)
+        s.max_dt = 5.0
+        big.append(s)
+    scns = (mixed_scenarios(workloads) if with_small else []) + big
+    with ensemble.Ensemble(scns) as ens:
+        ens.set_schedule(1)
+        ens.run(max_batch_steps=40)
+        for k, s in enumerate(scns):
+            info = ens.info(k)
+            assert info["status"] == 0 and info["steps"] > 0
+            with workloads.simulation_for(s) as sim:
+                sim.run_steps(info["steps"], s.t_end)
+                assert sim.steps() == info["steps"] and sim.time() == info["t"]
+                assert exact_fraction(ens.states(k), sim.states()) == 1.0, f"scenario {k}"

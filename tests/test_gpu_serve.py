@@ -79,3 +79,30 @@ def test_arrival_stream(gpu):
         ref, steps = alone(workloads, s)
         assert r.result["steps"] == steps
         assert exact_fraction(r.result["state"], ref) == 1.0
+
+
+def test_solo_scenarios_same_alone_and_in_the_mix(gpu):
+    """Scenarios of at least 512 tiles of 32 x 32 (736 x 736 and up) run their
+    stages as their own launches beside the batched ones; the graphs are
+    captured again whenever such a scenario is admitted or collected. Large
+    and small scenarios joining and leaving mid-flight: every result equals
+    its lone solve bit for bit."""
+    serve, workloads = gpu
+    big1, big2 = scn(workloads, 736, 11, 30.0, peak=200.0), scn(workloads, 768, 12, 20.0, peak=200.0)
+    small1, small2 = scn(workloads, 40, 13, 50.0), scn(workloads, 90, 14, 25.0)
+    results = {}
+    with serve.Server(hbm_budget_bytes=1 << 32, max_slots=8) as srv:
+        ids = {srv.try_admit(big1): "big1", srv.try_admit(small1): "small1"}
+        srv.advance(4)
+        ids[srv.try_admit(big2)] = "big2"     # a second large scenario joins mid-flight
+        while len(results) < 4:
+            srv.advance(3)
+            for slot in srv.finished():
+                results[ids[slot]] = srv.collect(slot)
+                if "small2" not in ids.values():
+                    ids[srv.try_admit(small2)] = "small2"
+    for name, s in (("big1", big1), ("big2", big2), ("small1", small1), ("small2", small2)):
+        r = results[name]
+        ref, steps = alone(workloads, s)
+        assert r["status"] == 0 and r["t"] == s.t_end and r["steps"] == steps, name
+        assert exact_fraction(r["state"], ref) == 1.0, name
