@@ -134,6 +134,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_stage_adj(const StageArgs A, co
     __syncthreads();
     for (int q = 0; q < CELLS_PER_THREAD; ++q) {
       const int li = tid / TX + ROWS_PER_PASS * q, lj = tid % TX;
+      if (kPartialPass && li >= TY) continue;
       const int gi = gi0 + li, gj = gj0 + lj;
       const int ce = icell(li, lj), c3 = i3(li, lj), c4 = i4(li, lj), ca = ia(li, lj);
       R.lprim[0][c3] = 0.0;  // bed-source adjoint of the cell's x / y eta slopes

@@ -29,7 +29,10 @@ namespace hf {
 // Both compute every cell with the same operations: results are identical.
 constexpr int TX = 32;
 constexpr int kGeomSmall = 0, kGeomLarge = 1;
-constexpr int kGeomTileH[2] = {8, 32};
+#ifndef HF_LARGE_TILE_Y
+#define HF_LARGE_TILE_Y 32  // the large geometry's tile height (build.py passes the same)
+#endif
+constexpr int kGeomTileH[2] = {8, HF_LARGE_TILE_Y};
 constexpr int kLargeTilesMin = 100;
 // A scenario of an ensemble or server with at least this many 32 x 32 tiles
 // (about 3.5 waves of the 148 SMs; from 724 x 724 cells on) fills the GPU
@@ -52,9 +55,13 @@ constexpr int kSoloTilesMin = 512;
 inline namespace HF_GEOM {
 constexpr int TY = HF_TILE_Y;
 constexpr int NTHREADS = HF_THREADS;
-constexpr int ROWS_PER_PASS = NTHREADS / TX;           // tile rows one pass of the CTA covers
-constexpr int CELLS_PER_THREAD = TX * TY / NTHREADS;   // cells a thread updates per tile
-static_assert(NTHREADS % TX == 0 && TY % ROWS_PER_PASS == 0, "tile / thread shape");
+constexpr int ROWS_PER_PASS = NTHREADS / TX;  // tile rows one pass of the CTA covers
+// Cells a thread updates per tile. When the tile height is not a multiple of
+// the rows of a pass, the last pass is partial (kPartialPass) and the threads
+// past the tile's last row skip it.
+constexpr int CELLS_PER_THREAD = (TY + ROWS_PER_PASS - 1) / ROWS_PER_PASS;
+constexpr bool kPartialPass = TY % ROWS_PER_PASS != 0;
+static_assert(NTHREADS % TX == 0, "tile / thread shape");
 static_assert(TY == kGeomTileH[HF_GEOM_INDEX], "geometry index and tile height");
 }  // namespace HF_GEOM
 

@@ -877,6 +877,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, StageSmemT<T>& S,
 #pragma unroll 1
     for (int q = 0; q < CELLS_PER_THREAD; ++q) {
       const int li = tid / TX + ROWS_PER_PASS * q, lj = tid % TX;
+      if (kPartialPass && li >= TY) continue;
       const int gi = gi0 + li, gj = gj0 + lj;
       if (!IN && (gi >= nr || gj >= nc)) continue;
       const int64_t g = (int64_t)gi * nc + gj;

@@ -334,6 +334,7 @@ __device__ void finalize_tiles(const StageArgs& A, Ctrl* ctrl, double& sxm, doub
       src_hi = A.f.tile_start[tile + 1];
     }
     for (int q = 0; q < CELLS_PER_THREAD; ++q) {
+      if (kPartialPass && (int)threadIdx.x / TX + ROWS_PER_PASS * q >= TY) continue;
       const int gi = gi0 + threadIdx.x / TX + ROWS_PER_PASS * q, gj = gj0 + threadIdx.x % TX;
       if (gi >= A.nr || gj >= A.nc) continue;
       const int64_t g = (int64_t)gi * A.nc + gj;
@@ -382,6 +383,7 @@ __global__ void __launch_bounds__(NTHREADS) k_cfl(const StageArgs A, int with_gh
     const int tyi = tile / A.tiles_x;
     const int gi0 = tyi * TY, gj0 = (tile - tyi * A.tiles_x) * TX;
     for (int q = 0; q < CELLS_PER_THREAD; ++q) {
+      if (kPartialPass && (int)threadIdx.x / TX + ROWS_PER_PASS * q >= TY) continue;
       const int gi = gi0 + threadIdx.x / TX + ROWS_PER_PASS * q, gj = gj0 + threadIdx.x % TX;
       if (gi >= A.nr || gj >= A.nc) continue;
       const int64_t g = (int64_t)gi * A.nc + gj;
@@ -409,6 +411,7 @@ __global__ void __launch_bounds__(NTHREADS)
     double sxm = 0.0, sym = 0.0;
     unsigned long long nonfin = 0;
     for (int q = 0; q < CELLS_PER_THREAD; ++q) {
+      if (kPartialPass && (int)threadIdx.x / TX + ROWS_PER_PASS * q >= TY) continue;
       const int gi = gi0 + threadIdx.x / TX + ROWS_PER_PASS * q, gj = gj0 + threadIdx.x % TX;
       if (gi >= A.nr || gj >= A.nc) continue;
       const int64_t g = (int64_t)gi * A.nc + gj;
