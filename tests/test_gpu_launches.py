@@ -56,3 +56,18 @@ def test_ensemble_launches_four_kernels_per_batch_step(gpu):
         e.run(72)  # one 64-step and one 8-step chunk
         assert _lib.kernel_launches() - before == 4 * 72
         assert all(e.info(k)["steps"] == 80 for k in range(2))
+
+
+def test_ensemble_solo_scenarios_add_two_launches_per_batch_step(gpu):
+    """A scenario of at least 512 tiles of 32 x 32 runs its two stages as its
+    own launches: 4 + 2 kernels per batch step with one such scenario."""
+    _lib, workloads = gpu
+    from hydroflux_b200.ensemble import Ensemble
+    scns = [workloads.valley(n=48, dx=5.0, seed=1, t_end=1e9),
+            workloads.valley(n=736, dx=5.0, seed=2, t_end=1e9)]
+    with Ensemble(scns) as e:
+        e.set_schedule(1)
+        e.run(8)
+        before = _lib.kernel_launches()
+        e.run(72)
+        assert _lib.kernel_launches() - before == 6 * 72
