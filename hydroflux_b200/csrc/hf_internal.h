@@ -349,8 +349,8 @@ int check_grid_config(const hf_config* cfg, int64_t nr, int64_t nc);
 int check_boundaries(const hf_boundaries& b, int64_t nr, int64_t nc);
 int check_grid_desc(const hf_grid* g);
 BcDev boundaries_dev(const hf_boundaries& b);
-// The error of this thread's last failed kernel launch in hf_kernels.cu's
-// launchers (they return -7 and keep the cudaError_t here).
+// The error of this thread's last failed kernel launch in the launchers
+// (launched() returns -7 and keeps the cudaError_t here).
 cudaError_t last_launch_error();
 // The error to report once a runtime call or a launcher has failed: the
 // runtime's pending error, else the launch error the launcher consumed, else

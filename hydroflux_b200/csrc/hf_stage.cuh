@@ -1,5 +1,5 @@
 // hf_stage.cuh -- the fused stage tile shared by the forward kernels
-// (hf_kernels.cu) and the adjoint kernels (hf_adjoint.cu): shared-memory
+// (hf_tiles.cu) and the adjoint kernels (hf_adjoint.cu): shared-memory
 // layout of a tile and its halo, the forward phases of one stage on a tile
 // (generic over the scalar: double or DualD), the per-cell epilogue
 // (friction, forcings) and the CFL reduction helpers.
