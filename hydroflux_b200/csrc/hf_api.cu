@@ -110,6 +110,36 @@ int dalloc(T** p, size_t n) {
 std::mutex g_pool_mu;
 cudaMemPool_t g_pool[64] = {};
 
+// Pinned host mirrors of control blocks (one Ctrl each) kept from destroyed
+// simulation handles for the next ones: pinning a fresh page costs 1-3 ms.
+// hf_release_cached_memory frees them.
+std::vector<Ctrl*> g_pinned_ctrl;
+constexpr size_t kPinnedCtrlKeep = 64;
+
+int pinned_ctrl_get(Ctrl** p) {
+  {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (!g_pinned_ctrl.empty()) {
+      *p = g_pinned_ctrl.back();
+      g_pinned_ctrl.pop_back();
+      return HF_OK;
+    }
+  }
+  return cuda_fail(cudaMallocHost((void**)p, sizeof(Ctrl)), "cudaMallocHost");
+}
+
+void pinned_ctrl_put(Ctrl* p) {
+  if (!p) return;
+  {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (g_pinned_ctrl.size() < kPinnedCtrlKeep) {
+      g_pinned_ctrl.push_back(p);
+      return;
+    }
+  }
+  cudaFreeHost(p);
+}
+
 int state_pool(int device, cudaMemPool_t* out) {
   if (device < 0 || device >= 64) return fail(HF_ERR_INVALID_ARG, "bad device index");
   std::lock_guard<std::mutex> lk(g_pool_mu);
@@ -557,9 +587,9 @@ void destroy_sim(hf_sim* s) {
   for (void* p : {(void*)s->d_z, (void*)s->d_n, (void*)s->d_h, (void*)s->d_hu, (void*)s->d_hv,
                   (void*)s->d_h1, (void*)s->d_hu1, (void*)s->d_hv1})
     pfree(p, s->stream);
-  dfree(s->d_ctrl);
+  pfree(s->d_ctrl, s->stream);
   if (s->stream) cudaStreamSynchronize(s->stream);  // the frees complete before the stream goes
-  if (s->h_ctrl) cudaFreeHost(s->h_ctrl);
+  pinned_ctrl_put(s->h_ctrl);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
 }
@@ -634,12 +664,14 @@ int hf_sim_create(const hf_mesh_desc* mesh, const double* h, const double* hu, c
   double** bufs[8] = {&s->d_z, &s->d_n, &s->d_h, &s->d_hu, &s->d_hv, &s->d_h1, &s->d_hu1, &s->d_hv1};
   for (double** b : bufs)
     if ((rc = palloc(b, (size_t)ncell, device, s->stream)) != HF_OK) return done(rc);
+  if ((rc = palloc(reinterpret_cast<double**>(&s->d_ctrl),
+                   (sizeof(Ctrl) + sizeof(double) - 1) / sizeof(double), device, s->stream)) !=
+      HF_OK)
+    return done(rc);
   // Stream-ordered allocations: usable from any stream once this completes.
   if (cudaStreamSynchronize(s->stream) != cudaSuccess)
     return done(cuda_fail(failed_call_error(), "pool allocation"));
-  if ((rc = dalloc(&s->d_ctrl, 1)) != HF_OK) return done(rc);
-  if (cudaMallocHost((void**)&s->h_ctrl, sizeof(Ctrl)) != cudaSuccess)
-    return done(cuda_fail(failed_call_error(), "cudaMallocHost"));
+  if ((rc = pinned_ctrl_get(&s->h_ctrl)) != HF_OK) return done(rc);
   const size_t bytes = (size_t)ncell * sizeof(double);
   if (cudaMemcpy(s->d_z, mesh->bed, bytes, cudaMemcpyHostToDevice) != cudaSuccess)
     return done(cuda_fail(failed_call_error(), "copy bed"));
@@ -1045,6 +1077,8 @@ int hf_sim_gauge_series(hf_sim* s, double* t, double* h, int64_t* n_stored, int6
 int hf_release_cached_memory(int device) {
   if (device < 0 || device >= 64) return fail(HF_ERR_INVALID_ARG, "bad device index");
   std::lock_guard<std::mutex> lk(g_pool_mu);
+  for (Ctrl* p : g_pinned_ctrl) cudaFreeHost(p);
+  g_pinned_ctrl.clear();
   if (!g_pool[device]) return HF_OK;
   DeviceGuard guard(device);
   HF_CUDA(cudaDeviceSynchronize());
