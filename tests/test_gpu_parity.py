@@ -389,3 +389,28 @@ def test_state_pool_reuse_and_release(gpu):
     live.close()
     for r in results[1:]:
         assert all(np.array_equal(a, b) for a, b in zip(r, results[0]))
+
+
+def test_free_functions_on_32x32_tiles_against_oracle(gpu, oracle):
+    """The free-function entry points take the 32 x 32 tile geometry from
+    100 such tiles on (here 352 x 330: 121 tiles, partial last tiles in both
+    directions): cfl_time_step_with_bcs and ssprk2_step give the oracle's
+    bits there too."""
+    sim, step = gpu
+    nr, nc = 352, 330
+    z, n, h, hu, hv = random_case(nr, nc, seed=4242)
+    pairs = BC_SETS["mixed"]
+    bcs_c = abi.make_boundaries(*pairs)
+    mesh = step.DeviceMesh(z, 1.5, 0.75, n)
+    ws = step.StepWorkspace2D(nr, nc)
+    dh, dhu, dhv = to_dev(h, hu, hv)
+    ref = (h, hu, hv)
+    for it in range(2):
+        dt_ref = oracle.cfl_time_step(z, 1.5, 0.75, *ref, 0.45, bcs=bcs_c, n=n)
+        dt_gpu = step.cfl_time_step_with_bcs(dh, dhu, dhv, mesh, bcs_obj(sim, pairs), 0.45, ws)
+        assert dt_gpu == dt_ref
+        dt = min(dt_ref, 0.05)
+        ref = oracle.ssprk2_step(z, 1.5, 0.75, *ref, bcs_c, dt, n)
+        step.ssprk2_step(dh, dhu, dhv, mesh, bcs_obj(sim, pairs), dt, ws)
+        got = to_host(dh, dhu, dhv)
+        assert exact_fraction(got, ref) == 1.0, f"step {it}: not bit-exact"
