@@ -22,7 +22,7 @@ namespace hf {
 //   calibration handle's runs use this geometry only.
 // - 32 x 32 (g32, kGeomLarge): 1024 threads, 211 KB of shared memory, one
 //   CTA (32 warps) per SM. The halo is a smaller share of the tile (2.32
-//   Audusse+HLLC faces and 2.36 limited-slope cells per cell against 2.83
+//   Audusse+HLLC faces and 2.39 limited-slope cells per cell against 2.83
 //   and 3.0) and an SM runs more warps; a stage launch on the 4096^2 valley
 //   takes 2.06 ms against 2.36 ms. Grids with at least kLargeTilesMin tiles
 //   of it take it (geom_for).

@@ -2,7 +2,9 @@
 //
 // k_stage_pf computes a 32 x 8 tile with a 4-cell halo from scratch: 2.83
 // Audusse+HLLC faces, 3.0 limited-slope cells and 2.1 primitive cells per
-// cell, most of the excess in the halo rows above and below the tile. Here a
+// cell, most of the excess in the halo rows above and below the tile (on
+// its 32 x 32 tiles: 2.32, 2.39 and 1.41). This kernel is built with the
+// 32 x 8 geometry's 256-thread CTAs only. Here a
 // CTA instead walks DOWN a 32-column strip in blocks of STRIP_ROWS (7) rows:
 // every array (depth, primitives, slopes, faces, alpha) keeps the rows the
 // next block shares with this one, which are shifted to the top of their
