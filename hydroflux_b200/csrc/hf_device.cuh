@@ -155,14 +155,8 @@ __device__ __forceinline__ void wb_face(T hL, T qnL, T qtL, T hR, T qnR, T qtR, 
   const T hsL = r_max(hL + zf - z_max, Z);
   const T hsR = r_max(hR + zf - z_max, Z);
   T unL = Z, utL = Z, unR = Z, utR = Z;
-  if (val(hL) > H_VEL) {
-    unL = dvp(qnL, hL);  // hL > H_VEL
-    utL = dvp(qtL, hL);
-  }
-  if (val(hR) > H_VEL) {
-    unR = dvp(qnR, hR);
-    utR = dvp(qtR, hR);
-  }
+  if (val(hL) > H_VEL) dvp2(qnL, qtL, hL, unL, utL);  // hL > H_VEL
+  if (val(hR) > H_VEL) dvp2(qnR, qtR, hR, unR, utR);
   T fm, fn, ft;
   hllc_normal<T>(hsL, hsL * unL, hsL * utL, hsR, hsR * unR, hsR * utR, fm, fn, ft);
   const T corrL = (hL * hL - hsL * hsL) * (0.5 * GRAVITY);

@@ -70,6 +70,21 @@ __device__ __forceinline__ DualD dvp(double a, DualD b) {
   return DualD{hfa::div_rn_pos(a, b.v), hfa::div_rn(-a * b.d, b.v * b.v)};
 }
 
+// Two quotients a1 / b and a2 / b by one divisor b > 0: the same correctly
+// rounded quotients as dvp. For f64 they share one division: the reciprocal
+// of b (hfa::make_recip) and Markstein's correction per numerator
+// (hfa::div_recip, which divides outright wherever that does not hold).
+// DualD divides each value and tangent as dvp does.
+__device__ __forceinline__ void dvp2(double a1, double a2, double b, double& q1, double& q2) {
+  const hfa::RecipD r = hfa::make_recip(b);
+  q1 = hfa::div_recip(a1, r);
+  q2 = hfa::div_recip(a2, r);
+}
+__device__ __forceinline__ void dvp2(DualD a1, DualD a2, DualD b, DualD& q1, DualD& q2) {
+  q1 = dvp(a1, b);
+  q2 = dvp(a2, b);
+}
+
 // Division by a grid spacing through its precomputed reciprocal (the same
 // correctly rounded quotient as dvp; hfa::div_recip).
 __device__ __forceinline__ double dvr(double a, const hfa::RecipD& r) {

@@ -602,10 +602,7 @@ __device__ __forceinline__ bool stage_tile_faces(const StageArgs& A, StageSmemT<
         const int k3 = (r - 1) * R3W + (cc - 1);
         const double zz = S.eta[k3], qu = S.u[k3], qv = S.v[k3];
         double uu = 0.0, vv = 0.0;
-        if (hh > H_VEL) {
-          uu = hfa::div_rn_pos(qu, hh);
-          vv = hfa::div_rn_pos(qv, hh);
-        }
+        if (hh > H_VEL) dvp2(qu, qv, hh, uu, vv);
         S.z[k3] = zz;
         S.eta[k3] = hh + zz;
         S.u[k3] = uu;
