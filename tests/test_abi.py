@@ -132,3 +132,25 @@ def test_python_mirror_errors_without_gpu(libpath):
         sim.Simulation(mesh, (np.ones((4, 4)),) * 3, sim.SimulationConfig(cfl=0.0))
     with pytest.raises(sim.ShapeMismatch):
         sim.Simulation(mesh, (np.ones((3, 3)),) * 3)
+
+
+def test_c99_consumer_compiles_links_and_runs(libpath):
+    """The header as a foreign binding sees it: a C99 program (no C++, no CUDA
+    headers) that includes it, links the library by name and calls the entry
+    points that need no GPU."""
+    import shutil
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("gcc not available")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = os.path.join(root, "tests", "native", "abi_consumer.c")
+    out_dir = os.path.join(root, "tests", "native", "_build")
+    os.makedirs(out_dir, exist_ok=True)
+    exe = os.path.join(out_dir, "abi_consumer")
+    libdir = os.path.dirname(libpath)
+    subprocess.run([gcc, "-std=c99", "-Wall", "-Wextra", "-Werror", "-pedantic", "-I",
+                    os.path.join(root, "include"), src, "-L", libdir, "-lhydroflux_gpu",
+                    f"-Wl,-rpath,{libdir}", "-o", exe], check=True)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    assert "abi consumer ok" in r.stdout
