@@ -5,7 +5,9 @@ Each scenario behaves like its own `Simulation` run to its horizon
 roughness, forcings, CFL dt, clock, step budget and errors. One batch step
 advances every unfinished scenario by one of its own steps with a single
 persistent launch per stage over the tiles of all scenarios (hf_batch_* in
-include/hydroflux_gpu.h). Results are bit-identical to separate solves.
+include/hydroflux_gpu.h); a scenario large enough to fill the GPU by itself
+(512 or more tiles of 32 x 32) runs its stages as its own launches in the
+same step. Results are bit-identical to separate solves.
 """
 from __future__ import annotations
 

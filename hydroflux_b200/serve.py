@@ -2,7 +2,8 @@
 
 Requests arrive over time; each is admitted into a slot as soon as a slot is
 free and its fields fit the HBM budget, then advances together with every
-other admitted scenario (one launch per stage over all their tiles). A
+other admitted scenario (one launch per stage over all their tiles; a
+scenario that fills the GPU by itself gets its own launches). A
 finished scenario is collected, freeing its slot and memory for the next
 request. `serve_stream` drives an arrival stream and reports per-request
 latency (arrival -> result) and throughput.
